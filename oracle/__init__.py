@@ -1,0 +1,175 @@
+"""CPU FP64 oracle for GIEM2G's integral-equation solve path.
+
+TEST INFRASTRUCTURE ONLY.  This package restates the reference's Fortran
+routines in C (``giem2g_oracle.c``) and exposes them through ctypes.  The
+product (``giem2g_b200``) never imports it; only ``tests/``, the smoke check and
+the benchmark's CPU-baseline leg do, as the checker.
+
+Parity status: the reference ships no tests or golden vectors and cannot be
+built in this environment (Fortran/MPI/FFTW), so parity against reference
+outputs is UNPINNED.  The oracle is anchored on a dense block-Toeplitz brute
+force and on an independent numpy restatement (tests/test_oracle.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liborc_giem2g.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc + OpenMP)."""
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "giem2g_oracle.c"))
+    ):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.orc_green_tensor.argtypes = [vp, vp, vp, ip]
+        L.orc_tensor_spectrum.argtypes = [ip, ip, ip, vp, vp, vp, vp, ip]
+        L.orc_apply.argtypes = [ip, ip, ip, vp, vp, vp, vp, vp, vp, vp, vp, ip]
+        L.orc_apply_toeplitz.argtypes = [ip, ip, ip, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_plane_wave.argtypes = [vp, ip, vp]
+        L.orc_solve.argtypes = [ip, ip, ip, vp, vp, vp, vp, vp, vp, vp, vp, ip, ip, ip, dp, vp, vp, vp, ip, ip]
+        L.orc_vbt_weights.argtypes = [dp, dp, dp, dp, dp, vp, vp]
+        L.orc_background_cells.argtypes = [vp, vp, vp]
+        L.orc_layer_numbers.argtypes = [vp, vp]
+        L.orc_eps0.restype = dp
+        L.orc_mu0.restype = dp
+        _lib = L
+    return _lib
+
+
+class _Model(ctypes.Structure):
+    _fields_ = [
+        ("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+        ("z", ctypes.c_void_p), ("Nl", ctypes.c_int),
+        ("csigma", ctypes.c_void_p), ("thick", ctypes.c_void_p), ("omega", ctypes.c_double),
+    ]
+
+
+class OrcResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("bea", ctypes.c_double), ("be", ctypes.c_double),
+                ("stat", ctypes.c_int), ("applies", ctypes.c_int)]
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c128(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _model_struct(m):
+    z = _f64(m.z)
+    cs = _c128(m.csigma)
+    th = _f64(m.thick) if len(m.thick) else np.zeros(1)
+    s = _Model(m.Nx, m.Ny, m.Nz, m.dx, m.dy, z.ctypes.data, m.Nl, cs.ctypes.data, th.ctypes.data, m.omega)
+    return s, (z, cs, th)
+
+
+def green_tensor(m, nthreads: int = 0):
+    """Spatial tensor: symm[Nx,Ny,4,P], asym[Nx,Ny,2,Nz*Nz] (calc_ie_tensor_module.F90:54)."""
+    P = m.Nz * (m.Nz + 1) // 2
+    symm = np.zeros((m.Nx, m.Ny, 4, P), np.complex128)
+    asym = np.zeros((m.Nx, m.Ny, 2, m.Nz * m.Nz), np.complex128)
+    s, keep = _model_struct(m)
+    lib().orc_green_tensor(ctypes.byref(s), _p(symm), _p(asym), nthreads)
+    return symm, asym
+
+
+def background_cells(m):
+    csigb = np.zeros(m.Nz, np.complex128)
+    sqsigb = np.zeros(m.Nz, np.float64)
+    s, keep = _model_struct(m)
+    lib().orc_background_cells(ctypes.byref(s), _p(csigb), _p(sqsigb))
+    return csigb, sqsigb
+
+
+def layer_numbers(m):
+    L = np.zeros(m.Nz + 1, np.int32)
+    s, keep = _model_struct(m)
+    lib().orc_layer_numbers(ctypes.byref(s), _p(L))
+    return L
+
+
+def tensor_spectrum(Nx, Ny, Nz, symm, asym, nthreads: int = 0):
+    symm, asym = _c128(symm), _c128(asym)
+    sh = np.zeros_like(symm)
+    ah = np.zeros_like(asym)
+    lib().orc_tensor_spectrum(Nx, Ny, Nz, _p(symm), _p(asym), _p(sh), _p(ah), nthreads)
+    return sh, ah
+
+
+def apply(Nx, Ny, Nz, sh, ah, csiga, csigb, sqsigb, dz, v_in, nthreads: int = 0):
+    sh, ah, csiga, csigb = _c128(sh), _c128(ah), _c128(csiga), _c128(csigb)
+    sqsigb, dz, v_in = _f64(sqsigb), _f64(dz), _c128(v_in)
+    out = np.zeros_like(v_in)
+    lib().orc_apply(Nx, Ny, Nz, _p(sh), _p(ah), _p(csiga), _p(csigb), _p(sqsigb), _p(dz), _p(v_in), _p(out), nthreads)
+    return out
+
+
+def apply_toeplitz(Nx, Ny, Nz, symm, asym, csiga, csigb, sqsigb, dz, v_in):
+    symm, asym, csiga, csigb = _c128(symm), _c128(asym), _c128(csiga), _c128(csigb)
+    sqsigb, dz, v_in = _f64(sqsigb), _f64(dz), _c128(v_in)
+    out = np.zeros_like(v_in)
+    lib().orc_apply_toeplitz(Nx, Ny, Nz, _p(symm), _p(asym), _p(csiga), _p(csigb), _p(sqsigb), _p(dz), _p(v_in), _p(out))
+    return out
+
+
+def plane_wave(m, pol: int):
+    """pol 0 = EX, 1 = EY.  Returns E0[3,Nz,Ny,Nx] (sources_module.F90:67)."""
+    E0 = np.zeros((3, m.Nz, m.Ny, m.Nx), np.complex128)
+    s, keep = _model_struct(m)
+    lib().orc_plane_wave(ctypes.byref(s), pol, _p(E0))
+    return E0
+
+
+def solve(Nx, Ny, Nz, sh, ah, csiga, csigb, sqsigb, dz, E_bkg, E0_guess=None, outer_buf=30, inner_buf=10,
+          max_restart=100, tol=1e-8, history_len=4096, nthreads: int = 0):
+    """SolveEquation (ie_solver_module.F90:43).  Returns (Esol, OrcResult, outer misfit history)."""
+    sh, ah, csiga, csigb = _c128(sh), _c128(ah), _c128(csiga), _c128(csigb)
+    sqsigb, dz, E_bkg = _f64(sqsigb), _f64(dz), _c128(E_bkg)
+    g = _c128(E0_guess) if E0_guess is not None else None
+    Esol = np.zeros_like(E_bkg)
+    info = OrcResult()
+    hist = np.zeros(history_len, np.float64)
+    lib().orc_solve(Nx, Ny, Nz, _p(sh), _p(ah), _p(csiga), _p(csigb), _p(sqsigb), _p(dz), _p(E_bkg),
+                    _p(g) if g is not None else None, outer_buf, inner_buf, max_restart, tol, _p(Esol),
+                    ctypes.byref(info), _p(hist), history_len, nthreads)
+    return Esol, info, hist[: max(0, min(info.iterations, history_len))].copy()
+
+
+def vbt_weights(x, y, hx, hy, rmin):
+    WT = np.zeros((501, 6), np.float64)
+    lms = np.zeros(501, np.float64)
+    lib().orc_vbt_weights(x, y, hx, hy, rmin, _p(WT), _p(lms))
+    return WT, lms
+
+
+def eps0() -> float:
+    return lib().orc_eps0()
+
+
+def mu0() -> float:
+    return lib().orc_mu0()
