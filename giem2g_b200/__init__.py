@@ -1,1 +1,284 @@
-"""B200-native IE-solve hot path of GIEM2G (placeholder, filled in below)."""
+"""B200-native implementation of GIEM2G's integral-equation solve path.
+
+The compute runs in ``_lib/libgiem2g_b200.so`` (hand-written sm_100a CUDA behind the C ABI
+declared in ``include/giem2g.h``).  This module is a thin ctypes host layer that mirrors
+the reference's Fortran module interface for the path:
+
+  IEOperator.set_anomaly_sigma   SetAnomalySigma   (ie_solver_module.F90:116)
+  IEOperator.calc_ie_kernel      CalcIntegralGreenTensor (calc_ie_tensor_module.F90:54)
+  IEOperator.calc_fft_of_ie_kernel CalcFFTofIETensor (Integral_Equation_Module.F90:310)
+  IEOperator.apply_precond       APPLY_PRECOND     (apply_ie_operator_module.F90:39)
+  IEOperator.solve_equation      SolveEquation     (ie_solver_module.F90:43)
+
+There is no CPU fallback: importing the library fails loudly if the extension is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_lib", "libgiem2g_b200.so")
+_lib = None
+
+CONVERGED, NON_TRUE_CONVERGED, NON_CONVERGED, INTERUPTED = 1, 2, -1, -3  # fgmres_interfaces.F90:25-30
+
+
+class Giem2gError(RuntimeError):
+    pass
+
+
+class BackgroundT(ctypes.Structure):      # giem2g_interfaces.F90:33-37
+    _fields_ = [("Nl", ctypes.c_int), ("csigb", ctypes.c_void_p), ("thickness", ctypes.c_void_p)]
+
+
+class AnomalyT(ctypes.Structure):         # giem2g_interfaces.F90:39-44
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("Nz", ctypes.c_int),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double),
+                ("z", ctypes.c_void_p), ("dz", ctypes.c_void_p)]
+
+
+class DataT(ctypes.Structure):            # giem2g_interfaces.F90:46-58
+    _fields_ = [("tensor_size", ctypes.c_longlong), ("ie_kernel_buffer_length", ctypes.c_longlong),
+                ("fft_buffers_length", ctypes.c_longlong), ("comm64", ctypes.c_longlong),
+                ("giem2g_tensor", ctypes.c_void_p), ("dz", ctypes.c_void_p), ("sqsigb", ctypes.c_void_p),
+                ("csigb", ctypes.c_void_p), ("kernel_buffer", ctypes.c_void_p),
+                ("fft_buffer_in", ctypes.c_void_p), ("fft_buffer_out", ctypes.c_void_p)]
+
+
+class FgmresCtl(ctypes.Structure):        # data_types_module.F90:49-55 (+ precision)
+    _fields_ = [("misfit", ctypes.c_double), ("fgmres_maxit", ctypes.c_int), ("gmres_buf", ctypes.c_int),
+                ("fgmres_buf", ctypes.c_int), ("precision", ctypes.c_int)]
+
+
+class ResultT(ctypes.Structure):          # fgmres_interfaces.F90:34-39 (+ counters)
+    _fields_ = [("iterations", ctypes.c_int), ("bea", ctypes.c_double), ("be", ctypes.c_double),
+                ("stat", ctypes.c_int), ("applies_fp64", ctypes.c_int), ("applies_fp32", ctypes.c_int),
+                ("device_ms", ctypes.c_double)]
+
+
+EXPORTED_SYMBOLS = [
+    "giem2g_calc_data_sizes", "giem2g_prepare_ie_kernel", "giem2g_calc_ie_kernel",
+    "giem2g_calc_fft_of_ie_kernel", "giem2g_set_anomaly_conductivity", "giem2g_apply_ie_operator",
+    "giem2g_set_logger", "giem2g_print_stats", "giem2g_delete_ie_operator",
+    "giem2g_last_status", "giem2g_last_error", "giem2g_set_background", "giem2g_set_ie_kernel_spatial",
+    "giem2g_get_ie_kernel_spatial", "giem2g_get_ie_kernel_spectral", "giem2g_apply_ie_operator_device",
+    "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_solve",
+    "giem2g_solve_device", "giem2g_get_misfit_history",
+]
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib():
+    """Load the CUDA library; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise Giem2gError(f"CUDA extension not built: {_LIB_PATH} missing (run giem2g_b200.build.build())")
+    L = ctypes.CDLL(_LIB_PATH)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.giem2g_calc_data_sizes.argtypes = [AnomalyT, ctypes.POINTER(DataT)]
+    L.giem2g_calc_data_sizes.restype = None
+    L.giem2g_prepare_ie_kernel.argtypes = [AnomalyT, DataT]
+    L.giem2g_prepare_ie_kernel.restype = None
+    L.giem2g_calc_ie_kernel.argtypes = [vp, BackgroundT, AnomalyT, dp]
+    L.giem2g_calc_ie_kernel.restype = None
+    L.giem2g_calc_fft_of_ie_kernel.argtypes = [vp]
+    L.giem2g_calc_fft_of_ie_kernel.restype = None
+    L.giem2g_set_anomaly_conductivity.argtypes = [vp, vp]
+    L.giem2g_set_anomaly_conductivity.restype = None
+    L.giem2g_apply_ie_operator.argtypes = [vp, vp, vp]
+    L.giem2g_apply_ie_operator.restype = None
+    L.giem2g_print_stats.argtypes = [vp]
+    L.giem2g_print_stats.restype = None
+    L.giem2g_delete_ie_operator.argtypes = [vp]
+    L.giem2g_delete_ie_operator.restype = None
+    L.giem2g_last_status.restype = ip
+    L.giem2g_last_error.restype = ctypes.c_char_p
+    L.giem2g_set_background.argtypes = [vp, BackgroundT, dp]
+    L.giem2g_set_ie_kernel_spatial.argtypes = [vp, vp, vp]
+    L.giem2g_get_ie_kernel_spatial.argtypes = [vp, vp, vp]
+    L.giem2g_get_ie_kernel_spectral.argtypes = [vp, vp, vp]
+    L.giem2g_apply_ie_operator_device.argtypes = [vp, vp, vp, ip]
+    L.giem2g_get_stream.argtypes = [vp]
+    L.giem2g_get_stream.restype = vp
+    L.giem2g_last_apply_ms.argtypes = [vp]
+    L.giem2g_last_apply_ms.restype = dp
+    L.giem2g_last_kernel_launches.argtypes = [vp]
+    L.giem2g_solve.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
+    L.giem2g_solve_device.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
+    L.giem2g_get_misfit_history.argtypes = [vp, vp, ip]
+    _lib = L
+    return L
+
+
+def _check(rc=None, what=""):
+    L = lib()
+    st = L.giem2g_last_status() if rc is None else rc
+    if st != 0:
+        raise Giem2gError(f"{what}: status {st}: {L.giem2g_last_error().decode(errors='replace')}")
+
+
+def _c128(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+@dataclass
+class SolveInfo:
+    iterations: int
+    bea: float
+    be: float
+    stat: int
+    applies_fp64: int
+    applies_fp32: int
+    device_ms: float
+    misfits: np.ndarray
+
+
+class IEOperator:
+    """One IE operator resident on the current CUDA device (IntegralEquationOperator)."""
+
+    def __init__(self, Nx, Ny, Nz, dx, dy, z):
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.dx, self.dy = float(dx), float(dy)
+        self._z = np.ascontiguousarray(z, dtype=np.float64)
+        self._dz = np.ascontiguousarray(np.diff(self._z), dtype=np.float64)
+        self._anom = AnomalyT(self.Nx, self.Ny, self.Nz, self.dx, self.dy, self._z.ctypes.data, self._dz.ctypes.data)
+        L = lib()
+        self._data = DataT()
+        L.giem2g_calc_data_sizes(self._anom, ctypes.byref(self._data))
+        _check(what="giem2g_calc_data_sizes")
+        L.giem2g_prepare_ie_kernel(self._anom, self._data)
+        _check(what="giem2g_prepare_ie_kernel")
+        self.handle = self._data.giem2g_tensor
+        self._keep = []
+
+    @classmethod
+    def from_model(cls, m):
+        return cls(m.Nx, m.Ny, m.Nz, m.dx, m.dy, m.z)
+
+    @property
+    def nvec(self):
+        return 3 * self.Nx * self.Ny * self.Nz
+
+    @property
+    def kernel_buffer_length(self):
+        return self._data.ie_kernel_buffer_length
+
+    def _bkg(self, csigma, thick):
+        cs = _c128(csigma)
+        th = np.ascontiguousarray(thick, dtype=np.float64) if len(thick) else np.zeros(1)
+        self._keep = [cs, th]
+        return BackgroundT(len(cs) - 1, cs.ctypes.data, th.ctypes.data)
+
+    def set_background(self, csigma, thick, omega):
+        _check(lib().giem2g_set_background(self.handle, self._bkg(csigma, thick), float(omega)), "giem2g_set_background")
+
+    def calc_ie_kernel(self, csigma, thick, omega):
+        """CalcIntegralGreenTensor on the GPU (FP64)."""
+        lib().giem2g_calc_ie_kernel(self.handle, self._bkg(csigma, thick), self._anom, float(omega))
+        _check(what="giem2g_calc_ie_kernel")
+
+    def set_ie_kernel_spatial(self, symm, asym):
+        s, a = _c128(symm), _c128(asym)
+        _check(lib().giem2g_set_ie_kernel_spatial(self.handle, s.ctypes.data, a.ctypes.data), "set_ie_kernel_spatial")
+
+    def get_ie_kernel_spatial(self):
+        P = self.Nz * (self.Nz + 1) // 2
+        s = np.zeros((self.Nx, self.Ny, 4, P), np.complex128)
+        a = np.zeros((self.Nx, self.Ny, 2, self.Nz * self.Nz), np.complex128)
+        _check(lib().giem2g_get_ie_kernel_spatial(self.handle, s.ctypes.data, a.ctypes.data), "get_ie_kernel_spatial")
+        return s, a
+
+    def get_ie_kernel_spectral(self):
+        P = self.Nz * (self.Nz + 1) // 2
+        s = np.zeros((self.Nx, self.Ny, 4, P), np.complex128)
+        a = np.zeros((self.Nx, self.Ny, 2, self.Nz * self.Nz), np.complex128)
+        _check(lib().giem2g_get_ie_kernel_spectral(self.handle, s.ctypes.data, a.ctypes.data), "get_ie_kernel_spectral")
+        return s, a
+
+    def calc_fft_of_ie_kernel(self):
+        lib().giem2g_calc_fft_of_ie_kernel(self.handle)
+        _check(what="giem2g_calc_fft_of_ie_kernel")
+
+    def set_anomaly_conductivity(self, csiga):
+        """csiga: complex [Nz,Ny,Nx] (Fortran (Nx,Ny,Nz))."""
+        c = _c128(csiga)
+        assert c.size == self.Nx * self.Ny * self.Nz
+        lib().giem2g_set_anomaly_conductivity(self.handle, c.ctypes.data)
+        _check(what="giem2g_set_anomaly_conductivity")
+
+    def set_anomaly_sigma(self, siga_file_order, freq, displacement_currents=True):
+        """SetAnomalySigma: real sigma in file order [Ny,Nx,Nz] -> csiga."""
+        from .synthetic import csiga_from_sigma
+        self.set_anomaly_conductivity(csiga_from_sigma(siga_file_order, freq, displacement_currents))
+
+    def apply_precond(self, v_in):
+        """APPLY_PRECOND through giem2g_apply_ie_operator (host arrays, complex128)."""
+        vi = _c128(v_in)
+        assert vi.size == self.nvec
+        vo = np.empty_like(vi)
+        lib().giem2g_apply_ie_operator(self.handle, vi.ctypes.data, vo.ctypes.data)
+        _check(what="giem2g_apply_ie_operator")
+        return vo
+
+    def apply_device(self, d_in: int, d_out: int, precision: int = 0):
+        _check(lib().giem2g_apply_ie_operator_device(self.handle, d_in, d_out, precision), "apply_device")
+
+    @property
+    def stream(self) -> int:
+        return lib().giem2g_get_stream(self.handle)
+
+    def last_apply_ms(self) -> float:
+        return lib().giem2g_last_apply_ms(self.handle)
+
+    def last_kernel_launches(self) -> int:
+        return lib().giem2g_last_kernel_launches(self.handle)
+
+    def _ctl(self, tol, max_restart, outer_buf, inner_buf, precision):
+        return FgmresCtl(float(tol), int(max_restart), int(inner_buf), int(outer_buf), int(precision))
+
+    def _info(self, r):
+        h = np.zeros(max(1, r.iterations), np.float64)
+        n = lib().giem2g_get_misfit_history(self.handle, h.ctypes.data, len(h))
+        return SolveInfo(r.iterations, r.bea, r.be, r.stat, r.applies_fp64, r.applies_fp32, r.device_ms, h[:n].copy())
+
+    def solve_equation(self, E_bkg, E0=None, tol=1e-8, max_restart=100, outer_buf=30, inner_buf=10, precision=0):
+        """SolveEquation with host arrays (Nx,Ny,Nz,3) complex128; returns (Esol, SolveInfo)."""
+        eb = _c128(E_bkg)
+        es = np.empty_like(eb)
+        e0 = _c128(E0) if E0 is not None else None
+        r = ResultT()
+        rc = lib().giem2g_solve(self.handle, eb.ctypes.data, es.ctypes.data, e0.ctypes.data if e0 is not None else None,
+                                self._ctl(tol, max_restart, outer_buf, inner_buf, precision), ctypes.byref(r))
+        _check(rc, "giem2g_solve")
+        return es, self._info(r)
+
+    def solve_device(self, d_ebkg: int, d_esol: int, d_e0=None, tol=1e-8, max_restart=100, outer_buf=30,
+                     inner_buf=10, precision=0):
+        r = ResultT()
+        rc = lib().giem2g_solve_device(self.handle, d_ebkg, d_esol, d_e0,
+                                       self._ctl(tol, max_restart, outer_buf, inner_buf, precision), ctypes.byref(r))
+        _check(rc, "giem2g_solve_device")
+        return self._info(r)
+
+    def print_stats(self):
+        lib().giem2g_print_stats(self.handle)
+
+    def delete(self):
+        if self.handle:
+            lib().giem2g_delete_ie_operator(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass

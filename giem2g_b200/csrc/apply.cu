@@ -1,0 +1,444 @@
+// IE operator apply on one GPU: y = sqrt(Re sb) * (a*x - IDFT2[ G_hat . DFT2(gsig*x) ] / (dz*4NxNy))
+//
+// Restates APPLY_PRECOND / MULT_IE_OP (apply_ie_operator_module.F90:39-263) without the MPI
+// slab decomposition: the padded 2Nx x 2Ny transform of the reference's Distributed_FFT.F90
+// becomes five kernels over HBM-resident buffers:
+//   k_fwd_x    pre-scale by gsig, zero-pad in x, forward x-FFT          x   -> U1[kx][zc][y]
+//   k_fwd_y    zero-pad in y, forward y-FFT, scatter to (q,r,slot)      U1  -> Uhat[q][r][4][zc]
+//   k_contract per (q,r): 6 Green's blocks applied to the 4 points (+-kx,+-ky)   Uhat in place
+//   k_bwd_y    inverse y-FFT, crop y<Ny                                 Uhat -> U1
+//   k_bwd_x    inverse x-FFT, crop x<Nx, post-combine                   U1  -> y
+// (kx-pair q, ky-pair r, slot s) <-> (kx,ky): kx = q (s&2==0) or 2Nx-q, with q=0,s&2 the x-Nyquist;
+// ky = r (s&1==0) or 2Ny-r, with r=0,s&1 the y-Nyquist.  Nyquist outputs are zero as in the
+// reference (FinalTransposeRepack / DistributedFourierYRepack drop them).
+#include <type_traits>
+#include "common.cuh"
+#include "ie_internal.h"
+
+namespace {
+
+template <typename R> using CT = typename Cplx<R>::T;
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------------------------
+// k_fwd_x: one CTA = TY consecutive y rows of one (z,c) line set.  apply_ie_operator_module.F90:57-115
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_fwd_x(const CT<R> *__restrict__ vin, const CT<R> *__restrict__ gsig,
+                                                    CT<R> *__restrict__ U1, const CT<R> *__restrict__ tw, int Nx,
+                                                    int Ny, int Nz, int TY)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
+    const int L = 2 * Nx, lg = ilog2(L), ls = L + 1;
+    const int y0 = blockIdx.x * TY, zc = blockIdx.y, z = zc % Nz;
+    const int nl = min(TY, Ny - y0);
+    const size_t plane = (size_t)Nx * Ny;
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+        const int t = i / L, x = i - t * L;
+        CT<R> v = czero<CT<R>>();
+        if (x < Nx) {
+            const size_t cell = (size_t)z * plane + (size_t)(y0 + t) * Nx + x;
+            v = cmul(vin[(size_t)zc * plane + (size_t)(y0 + t) * Nx + x], gsig[cell]);
+        }
+        s[t * ls + bitrev(x, lg)] = v;
+    }
+    __syncthreads();
+    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, false);
+    const int Z3 = 3 * Nz;
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+        const int kx = i / nl, t = i - kx * nl;
+        U1[((size_t)kx * Z3 + zc) * Ny + y0 + t] = s[t * ls + kx];
+    }
+}
+
+// slot helpers
+G2_D void kx_to_slot(int kx, int Nx, int &q, int &sx)
+{
+    if (kx < Nx) { q = kx; sx = 0; }
+    else if (kx == Nx) { q = 0; sx = 1; }
+    else { q = 2 * Nx - kx; sx = 1; }
+}
+G2_D void ky_to_slot(int ky, int Ny, int &r, int &sy)
+{
+    if (ky < Ny) { r = ky; sy = 0; }
+    else if (ky == Ny) { r = 0; sy = 1; }
+    else { r = 2 * Ny - ky; sy = 1; }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_fwd_y: one CTA = one kx column x TC (z,c) lines.  Distributed_FFT.F90:437-505 (y part + repack)
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_fwd_y(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uhat,
+                                                    const CT<R> *__restrict__ tw, int Nx, int Ny, int Nz, int TC)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
+    const int L = 2 * Ny, lg = ilog2(L), ls = L + 1, Z3 = 3 * Nz;
+    const int kx = blockIdx.x, zc0 = blockIdx.y * TC;
+    const int nl = min(TC, Z3 - zc0);
+    int q, sx;
+    kx_to_slot(kx, Nx, q, sx);
+    if (kx == Nx) {  // x-Nyquist column: never used, keep it zero
+        for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+            const int ky = i / nl, t = i - ky * nl;
+            int r, sy;
+            ky_to_slot(ky, Ny, r, sy);
+            Uhat[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = czero<CT<R>>();
+        }
+        return;
+    }
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+        const int t = i / L, y = i - t * L;
+        CT<R> v = czero<CT<R>>();
+        if (y < Ny) v = U1[((size_t)kx * Z3 + zc0 + t) * Ny + y];
+        s[t * ls + bitrev(y, lg)] = v;
+    }
+    __syncthreads();
+    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, false);
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+        const int ky = i / nl, t = i - ky * nl;
+        int r, sy;
+        ky_to_slot(ky, Ny, r, sy);
+        Uhat[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = s[t * ls + ky];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_contract: one CTA per (q,r).  apply_ie_operator_module.F90:265-374 (VERTICAL_MULT_GENERAL[_ZERO]).
+// Thread t < 3Nz owns output row (c,z) for the 4 points.  Tensor unit in smem:
+//   [xx P][xy P][yy P][zz P] packed upper (i<=j -> i + j(j+1)/2), [xz Nz*Nz][yz Nz*Nz] column-major.
+// Point signs (sigma_x, m) from slot s: sigma_x = -1 if s&2, m = -1 if s&1:
+//   xy: sigma_x*m   xz: sigma_x   zx: -sigma_x (xz^T)   yz: m   zy: -m (yz^T)   diagonal blocks: +1
+template <typename R>
+__global__ void k_contract(const CT<R> *__restrict__ G, CT<R> *__restrict__ Uhat, int Nx, int Ny, int Nz)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int P = Nz * (Nz + 1) / 2, T = 4 * P + 2 * Nz * Nz, Z3 = 3 * Nz;
+    CT<R> *sg = reinterpret_cast<CT<R> *>(smem_raw);
+    CT<R> *su = sg + T;  // [4][3Nz]
+    const size_t unit = blockIdx.x;
+    const int q = (int)(unit / Ny), r = (int)(unit - (size_t)q * Ny);
+    {
+        // 16-byte vector copy of the tensor unit
+        const int nbytes = T * (int)sizeof(CT<R>);
+        const int4 *src = reinterpret_cast<const int4 *>(G + unit * T);
+        int4 *dst = reinterpret_cast<int4 *>(sg);
+        // T = 2Nz(2Nz+1) is even, so every unit starts on a 16-byte boundary for both precisions
+        for (int i = threadIdx.x; i < nbytes / 16; i += blockDim.x) dst[i] = __ldcs(src + i);
+        for (int i = threadIdx.x; i < 4 * Z3; i += blockDim.x) su[i] = Uhat[unit * 4 * Z3 + i];
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t >= Z3) return;
+    const int c = t / Nz, z = t - c * Nz;
+    CT<R> acc[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) acc[p] = czero<CT<R>>();
+    for (int cp = 0; cp < 3; cp++) {
+        CT<R> part[4];
+#pragma unroll
+        for (int p = 0; p < 4; p++) part[p] = czero<CT<R>>();
+        // block selection
+        int kind;  // 0: symmetric packed, 1: asym (z,z'), 2: asym transposed (z',z)
+        const CT<R> *blk;
+        if (c == 0 && cp == 0) { kind = 0; blk = sg + 0 * P; }
+        else if ((c == 0 && cp == 1) || (c == 1 && cp == 0)) { kind = 0; blk = sg + 1 * P; }
+        else if (c == 1 && cp == 1) { kind = 0; blk = sg + 2 * P; }
+        else if (c == 2 && cp == 2) { kind = 0; blk = sg + 3 * P; }
+        else if (c == 0 && cp == 2) { kind = 1; blk = sg + 4 * P; }
+        else if (c == 1 && cp == 2) { kind = 1; blk = sg + 4 * P + Nz * Nz; }
+        else if (c == 2 && cp == 0) { kind = 2; blk = sg + 4 * P; }
+        else { kind = 2; blk = sg + 4 * P + Nz * Nz; }
+        const CT<R> *u = su + cp * Nz;
+        for (int zp = 0; zp < Nz; zp++) {
+            CT<R> g;
+            if (kind == 0) g = (z <= zp) ? blk[z + zp * (zp + 1) / 2] : blk[zp + z * (z + 1) / 2];
+            else if (kind == 1) g = blk[z + zp * Nz];
+            else g = blk[zp + z * Nz];
+#pragma unroll
+            for (int p = 0; p < 4; p++) cfma(part[p], g, u[p * Z3 + zp]);
+        }
+        // signs
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            const R sxs = (p & 2) ? R(-1) : R(1), ms = (p & 1) ? R(-1) : R(1);
+            R sg_ = R(1);
+            if ((c == 0 && cp == 1) || (c == 1 && cp == 0)) sg_ = sxs * ms;
+            else if (c == 0 && cp == 2) sg_ = sxs;
+            else if (c == 2 && cp == 0) sg_ = -sxs;
+            else if (c == 1 && cp == 2) sg_ = ms;
+            else if (c == 2 && cp == 1) sg_ = -ms;
+            acc[p].x += sg_ * part[p].x;
+            acc[p].y += sg_ * part[p].y;
+        }
+    }
+    if (q == 0) { acc[2] = czero<CT<R>>(); acc[3] = czero<CT<R>>(); }
+    if (r == 0) { acc[1] = czero<CT<R>>(); acc[3] = czero<CT<R>>(); }
+#pragma unroll
+    for (int p = 0; p < 4; p++) Uhat[unit * 4 * Z3 + p * Z3 + t] = acc[p];
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_bwd_y: inverse y-FFT of one kx column x TC lines, crop y < Ny.  Distributed_FFT.F90:696-788 + :455-476
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_bwd_y(const CT<R> *__restrict__ Uhat, CT<R> *__restrict__ U1,
+                                                    const CT<R> *__restrict__ tw, int Nx, int Ny, int Nz, int TC)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
+    const int L = 2 * Ny, lg = ilog2(L), ls = L + 1, Z3 = 3 * Nz;
+    const int kx = blockIdx.x, zc0 = blockIdx.y * TC;
+    const int nl = min(TC, Z3 - zc0);
+    if (kx == Nx) return;  // x-Nyquist column is not read by k_bwd_x
+    int q, sx;
+    kx_to_slot(kx, Nx, q, sx);
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+        const int ky = i / nl, t = i - ky * nl;
+        int r, sy;
+        ky_to_slot(ky, Ny, r, sy);
+        s[t * ls + bitrev(ky, lg)] = Uhat[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t];
+    }
+    __syncthreads();
+    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, true);
+    for (int i = threadIdx.x; i < nl * Ny; i += blockDim.x) {
+        const int t = i / Ny, y = i - t * Ny;
+        U1[((size_t)kx * Z3 + zc0 + t) * Ny + y] = s[t * ls + y];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_bwd_x: inverse x-FFT, crop x < Nx, post-combine.  apply_ie_operator_module.F90:125-174
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_bwd_x(const CT<R> *__restrict__ U1, const CT<R> *__restrict__ vin,
+                                                    const CT<R> *__restrict__ asig, const R *__restrict__ post,
+                                                    CT<R> *__restrict__ vout, const CT<R> *__restrict__ tw, int Nx,
+                                                    int Ny, int Nz, int TY)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
+    const int L = 2 * Nx, lg = ilog2(L), ls = L + 1, Z3 = 3 * Nz;
+    const int y0 = blockIdx.x * TY, zc = blockIdx.y, z = zc % Nz;
+    const int nl = min(TY, Ny - y0);
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
+        const int kx = i / nl, t = i - kx * nl;
+        CT<R> v = czero<CT<R>>();
+        if (kx != Nx) v = U1[((size_t)kx * Z3 + zc) * Ny + y0 + t];
+        s[t * ls + bitrev(kx, lg)] = v;
+    }
+    __syncthreads();
+    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, true);
+    const size_t plane = (size_t)Nx * Ny;
+    const R sq = post[z], inv = post[Nz + z];
+    for (int i = threadIdx.x; i < nl * Nx; i += blockDim.x) {
+        const int t = i / Nx, x = i - t * Nx;
+        const size_t cell = (size_t)z * plane + (size_t)(y0 + t) * Nx + x;
+        const size_t idx = (size_t)zc * plane + (size_t)(y0 + t) * Nx + x;
+        CT<R> d1 = cmul(vin[idx], asig[cell]);
+        CT<R> w = s[t * ls + x];
+        CT<R> o;
+        o.x = (d1.x - w.x * inv) * sq;
+        o.y = (d1.y - w.y * inv) * sq;
+        vout[idx] = o;
+    }
+}
+
+// per-cell coefficients (apply_ie_operator_module.F90:66-68, :134):
+//   asiga = 2*sqrt(Re sb)/(csiga + conj(sb)),  gsig = (csiga - sb)*asiga
+__global__ void k_sigma(const double2 *__restrict__ csiga, const double2 *__restrict__ csigb,
+                        const double *__restrict__ sq, double2 *gsig64, double2 *asig64, float2 *gsig32,
+                        float2 *asig32, size_t plane, int Nz)
+{
+    const size_t n = plane * Nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int z = (int)(i / plane);
+        const double2 sa = csiga[i], sb = csigb[z];
+        const double2 a = cdiv(make_double2(2.0 * sq[z], 0.0), make_double2(sa.x + sb.x, sa.y - sb.y));
+        const double2 g = cmul(make_double2(sa.x - sb.x, sa.y - sb.y), a);
+        gsig64[i] = g;
+        asig64[i] = a;
+        gsig32[i] = make_float2((float)g.x, (float)g.y);
+        asig32[i] = make_float2((float)a.x, (float)a.y);
+    }
+}
+
+template <typename R> struct Bufs;
+template <> struct Bufs<double> {
+    static const double2 *G(IeOp *o) { return o->d_tensor64; }
+    static const double2 *gsig(IeOp *o) { return o->d_gsig64; }
+    static const double2 *asig(IeOp *o) { return o->d_asig64; }
+    static const double *post(IeOp *o) { return o->d_post64; }
+    static const double2 *twx(IeOp *o) { return o->d_twx64; }
+    static const double2 *twy(IeOp *o) { return o->d_twy64; }
+};
+template <> struct Bufs<float> {
+    static const float2 *G(IeOp *o) { return o->d_tensor32; }
+    static const float2 *gsig(IeOp *o) { return o->d_gsig32; }
+    static const float2 *asig(IeOp *o) { return o->d_asig32; }
+    static const float *post(IeOp *o) { return o->d_post32; }
+    static const float2 *twx(IeOp *o) { return o->d_twx32; }
+    static const float2 *twy(IeOp *o) { return o->d_twy32; }
+};
+
+int pick_lines(int L, size_t elem, int maxlines)
+{
+    // lines per CTA such that the tile stays <= 64 KB of shared memory
+    int n = (int)((64 * 1024) / ((size_t)(L + 1) * elem));
+    if (n < 1) n = 1;
+    if (n > maxlines) n = maxlines;
+    return n;
+}
+
+}  // namespace
+
+int ie_kernel_launch_count_apply() { return 5; }
+
+template <typename R>
+static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st)
+{
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
+    const size_t es = sizeof(CT<R>);
+    CT<R> *U1 = reinterpret_cast<CT<R> *>(op->scratch.U1);
+    CT<R> *Uh = reinterpret_cast<CT<R> *>(op->scratch.Uhat);
+    const CT<R> *G = Bufs<R>::G(op);
+    if (!G || !U1 || !Uh) return G2_ERR_STATE;
+    // forward x
+    {
+        const int L = 2 * Nx, TY = pick_lines(L, es, 32);
+        const size_t sm = (size_t)TY * (L + 1) * es;
+        dim3 grid((Ny + TY - 1) / TY, Z3);
+        k_fwd_x<R><<<grid, kThreads, sm, st>>>(d_in, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, TY);
+    }
+    // forward y
+    {
+        const int L = 2 * Ny, TC = pick_lines(L, es, 32);
+        const size_t sm = (size_t)TC * (L + 1) * es;
+        dim3 grid(2 * Nx, (Z3 + TC - 1) / TC);
+        k_fwd_y<R><<<grid, kThreads, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, TC);
+    }
+    // contraction
+    {
+        const int T = op->Tunit();
+        const size_t sm = ((size_t)T + 4 * Z3) * es;
+        const int threads = ((Z3 + 31) / 32) * 32;
+        k_contract<R><<<(unsigned)op->units(), threads, sm, st>>>(G, Uh, Nx, Ny, Nz);
+    }
+    // inverse y
+    {
+        const int L = 2 * Ny, TC = pick_lines(L, es, 32);
+        const size_t sm = (size_t)TC * (L + 1) * es;
+        dim3 grid(2 * Nx, (Z3 + TC - 1) / TC);
+        k_bwd_y<R><<<grid, kThreads, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, TC);
+    }
+    // inverse x + post
+    {
+        const int L = 2 * Nx, TY = pick_lines(L, es, 32);
+        const size_t sm = (size_t)TY * (L + 1) * es;
+        dim3 grid((Ny + TY - 1) / TY, Z3);
+        k_bwd_x<R><<<grid, kThreads, sm, st>>>(U1, d_in, Bufs<R>::asig(op), Bufs<R>::post(op), d_out,
+                                               Bufs<R>::twx(op), Nx, Ny, Nz, TY);
+    }
+    G2_CUDA_CHECK(cudaGetLastError());
+    return G2_OK;
+}
+
+int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st)
+{
+    return ie_apply_device<double>(op, d_in, d_out, st);
+}
+int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st)
+{
+    return ie_apply_device<float>(op, d_in, d_out, st);
+}
+
+static int set_smem_attrs(IeOp *op)
+{
+    static bool done = false;
+    if (done) return G2_OK;
+    const int big = 227 * 1024;
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_x<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_x<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_contract<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_contract<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_x<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_x<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    (void)op;
+    done = true;
+    return G2_OK;
+}
+
+int ie_alloc_scratch(IeOp *op)
+{
+    const size_t n_u1 = (size_t)2 * op->Nx * 3 * op->Nz * op->Ny;
+    const size_t n_uh = (size_t)op->Nx * op->Ny * 4 * 3 * op->Nz;
+    if (!op->scratch.U1) G2_CUDA_CHECK(cudaMalloc(&op->scratch.U1, n_u1 * sizeof(double2)));
+    if (!op->scratch.Uhat) G2_CUDA_CHECK(cudaMalloc(&op->scratch.Uhat, n_uh * sizeof(double2)));
+    return set_smem_attrs(op);
+}
+
+// twiddles exp(-2 pi i j / L), j < L/2, rounded from long double
+static int make_tw(int L, double2 **d64, float2 **d32)
+{
+    std::vector<double2> h64(L / 2);
+    std::vector<float2> h32(L / 2);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int j = 0; j < L / 2; j++) {
+        long double a = -2.0L * pi * (long double)j / (long double)L;
+        h64[j] = make_double2((double)cosl(a), (double)sinl(a));
+        h32[j] = make_float2((float)cosl(a), (float)sinl(a));
+    }
+    G2_CUDA_CHECK(cudaMalloc(d64, sizeof(double2) * (L / 2)));
+    G2_CUDA_CHECK(cudaMalloc(d32, sizeof(float2) * (L / 2)));
+    G2_CUDA_CHECK(cudaMemcpy(*d64, h64.data(), sizeof(double2) * (L / 2), cudaMemcpyHostToDevice));
+    G2_CUDA_CHECK(cudaMemcpy(*d32, h32.data(), sizeof(float2) * (L / 2), cudaMemcpyHostToDevice));
+    return G2_OK;
+}
+
+int ie_make_twiddles(IeOp *op)
+{
+    int rc = make_tw(2 * op->Nx, &op->d_twx64, &op->d_twx32);
+    if (rc) return rc;
+    return make_tw(2 * op->Ny, &op->d_twy64, &op->d_twy32);
+}
+
+int ie_prepare_sigma(IeOp *op, cudaStream_t st)
+{
+    const int Nz = op->Nz;
+    const size_t n = op->cells();
+    if (!op->d_gsig64) {
+        G2_CUDA_CHECK(cudaMalloc(&op->d_gsig64, n * sizeof(double2)));
+        G2_CUDA_CHECK(cudaMalloc(&op->d_asig64, n * sizeof(double2)));
+        G2_CUDA_CHECK(cudaMalloc(&op->d_gsig32, n * sizeof(float2)));
+        G2_CUDA_CHECK(cudaMalloc(&op->d_asig32, n * sizeof(float2)));
+        G2_CUDA_CHECK(cudaMalloc(&op->d_post64, 2 * Nz * sizeof(double)));
+        G2_CUDA_CHECK(cudaMalloc(&op->d_post32, 2 * Nz * sizeof(float)));
+    }
+    std::vector<double> post(2 * Nz);
+    std::vector<float> post32(2 * Nz);
+    const double N = 4.0 * op->Nx * op->Ny;
+    for (int z = 0; z < Nz; z++) {
+        post[z] = op->sqsigb[z];
+        post[Nz + z] = 1.0 / (op->dz[z] * N);
+        post32[z] = (float)post[z];
+        post32[Nz + z] = (float)post[Nz + z];
+    }
+    G2_CUDA_CHECK(cudaMemcpyAsync(op->d_post64, post.data(), 2 * Nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    G2_CUDA_CHECK(cudaMemcpyAsync(op->d_post32, post32.data(), 2 * Nz * sizeof(float), cudaMemcpyHostToDevice, st));
+    double2 *d_csigb = nullptr;
+    double *d_sq = nullptr;
+    G2_CUDA_CHECK(cudaMalloc(&d_csigb, Nz * sizeof(double2)));
+    G2_CUDA_CHECK(cudaMalloc(&d_sq, Nz * sizeof(double)));
+    G2_CUDA_CHECK(cudaMemcpyAsync(d_csigb, op->csigb.data(), Nz * sizeof(double2), cudaMemcpyHostToDevice, st));
+    G2_CUDA_CHECK(cudaMemcpyAsync(d_sq, op->sqsigb.data(), Nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_sigma<<<592, 256, 0, st>>>(op->d_csiga, d_csigb, d_sq, op->d_gsig64, op->d_asig64, op->d_gsig32, op->d_asig32,
+                                 (size_t)op->Nx * op->Ny, Nz);
+    G2_CUDA_CHECK(cudaGetLastError());
+    G2_CUDA_CHECK(cudaStreamSynchronize(st));
+    cudaFree(d_csigb);
+    cudaFree(d_sq);
+    return G2_OK;
+}

@@ -1,0 +1,384 @@
+// C ABI: the reference's giem2g_* entry points (giem2g_interfaces.F90:76-254) plus extensions.
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include "common.cuh"
+#include "ie_internal.h"
+#include "krylov.h"
+
+namespace {
+std::mutex g_mu;
+std::string g_last_error;
+int g_last_status = 0;
+void (*g_logger)(const char *) = nullptr;
+IeOp *g_last_op = nullptr;  // giem2g_interfaces.F90:69 keeps the last operator in tmp_ptr
+
+int set_status(int rc)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_status = rc;
+    if (rc == 0) g_last_error.clear();
+    return rc;
+}
+IeOp *resolve(void *ie)
+{
+    // The reference's set_anomaly_conductivity/apply ignore their handle and use the last
+    // operator (giem2g_interfaces.F90:196,212); a NULL handle selects that one here.
+    return ie ? reinterpret_cast<IeOp *>(ie) : g_last_op;
+}
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// data_types_module.F90:214-242 GetLayerSingle; depth[1..Nl-1]
+int get_layer(double z, int Nl, const std::vector<double> &depth)
+{
+    if (std::fabs(z) < 1e-15) return 0;
+    if (z < 0) return -1;
+    if (Nl == 1) return 1;
+    int l = 1;
+    if (z > depth[Nl - 1]) return Nl;
+    while (z > depth[l]) l++;
+    return l;
+}
+}  // namespace
+
+void g2_log(const char *msg)
+{
+    if (g_logger) g_logger(msg);
+    else std::fprintf(stdout, "%s\n", msg);
+}
+void g2_set_error_msg(const std::string &msg)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error = msg;
+}
+void g2_set_error(const char *file, int line, const char *msg)
+{
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s:%d: %s", file, line, msg);
+    g2_set_error_msg(buf);
+}
+
+static int fail(int rc, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g2_set_error_msg(buf);
+    return set_status(rc);
+}
+
+extern "C" {
+
+int giem2g_last_status(void) { return g_last_status; }
+const char *giem2g_last_error(void) { return g_last_error.c_str(); }
+
+void giem2g_calc_data_sizes(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE *data)
+{
+    if (!data || anomaly.Nx <= 0 || anomaly.Ny <= 0 || anomaly.Nz <= 0) {
+        fail(G2_ERR_ARG, "giem2g_calc_data_sizes: bad anomaly shape");
+        return;
+    }
+    const long long Nx = anomaly.Nx, Ny = anomaly.Ny, Nz = anomaly.Nz;
+    data->tensor_size = (long long)sizeof(IeOp) / 8;
+    // CalcLocalKernelSize with every lag on one process (Integral_Equation_Module.F90:105-129)
+    data->ie_kernel_buffer_length = (2 * Nz * (Nz + 1) + 2 * Nz * Nz) * Nx * Ny;
+    // CalcLocalFFTSize(2Nx,2Ny,3Nz,1) (Distributed_FFT.F90:895-912)
+    data->fft_buffers_length = 2 * Nx * 3 * Nz * 2 * Ny;
+    IeOp *op = new IeOp();
+    op->Nx = anomaly.Nx;
+    op->Ny = anomaly.Ny;
+    op->Nz = anomaly.Nz;
+    g_last_op = op;
+    data->giem2g_tensor = op;
+    set_status(0);
+}
+
+void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data)
+{
+    IeOp *op = reinterpret_cast<IeOp *>(data.giem2g_tensor);
+    if (!op) { fail(G2_ERR_ARG, "giem2g_prepare_ie_kernel: no operator (call giem2g_calc_data_sizes first)"); return; }
+    const int Nx = anomaly.Nx, Ny = anomaly.Ny, Nz = anomaly.Nz;
+    if (!is_pow2(2 * Nx) || !is_pow2(2 * Ny) || 2 * Nx < 4 || 2 * Ny < 4 || 2 * Nx > 1024 || 2 * Ny > 1024) {
+        fail(G2_ERR_UNSUPPORTED, "giem2g_prepare_ie_kernel: 2*Nx and 2*Ny must be powers of two in [4,1024] (got Nx=%d Ny=%d)", Nx, Ny);
+        return;
+    }
+    const int Tmax_c128 = (227 * 1024) / 16 - 12 * Nz;
+    if (Nz < 1 || 2 * Nz * (2 * Nz + 1) > Tmax_c128) {
+        fail(G2_ERR_UNSUPPORTED, "giem2g_prepare_ie_kernel: Nz=%d exceeds the contraction tile limit", Nz);
+        return;
+    }
+    if (!anomaly.z) { fail(G2_ERR_ARG, "giem2g_prepare_ie_kernel: z is NULL"); return; }
+    op->Nx = Nx;
+    op->Ny = Ny;
+    op->Nz = Nz;
+    op->dx = anomaly.dx;
+    op->dy = anomaly.dy;
+    const double *z = reinterpret_cast<const double *>(anomaly.z);
+    op->z.assign(z, z + Nz + 1);
+    op->dz.resize(Nz);
+    for (int i = 0; i < Nz; i++) op->dz[i] = anomaly.dz ? reinterpret_cast<const double *>(anomaly.dz)[i] : z[i + 1] - z[i];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { fail(G2_ERR_CUDA, "no CUDA device"); return; }
+    if (!op->stream && cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        fail(G2_ERR_CUDA, "cudaStreamCreate failed");
+        return;
+    }
+    cudaEventCreate(&op->ev0);
+    cudaEventCreate(&op->ev1);
+    int rc = ie_make_twiddles(op);
+    if (!rc) rc = ie_alloc_scratch(op);
+    if (!rc && !op->d_csiga && cudaMalloc(&op->d_csiga, op->cells() * sizeof(double2)) != cudaSuccess) rc = G2_ERR_NOMEM;
+    if (!rc && !op->d_vin) {
+        if (cudaMalloc(&op->d_vin, op->nvec() * sizeof(double2)) != cudaSuccess ||
+            cudaMalloc(&op->d_vout, op->nvec() * sizeof(double2)) != cudaSuccess)
+            rc = G2_ERR_NOMEM;
+    }
+    if (rc) { fail(rc, "giem2g_prepare_ie_kernel: allocation failed (%s)", giem2g_last_error()); return; }
+    g_last_op = op;
+    set_status(0);
+}
+
+int giem2g_set_background(void *ie, GIEM2G_BACKGROUND_TYPE bkg, double omega)
+{
+    IeOp *op = resolve(ie);
+    if (!op || op->z.empty()) return fail(G2_ERR_STATE, "giem2g_set_background: operator not prepared");
+    if (bkg.Nl < 1 || !bkg.csigb || (bkg.Nl > 1 && !bkg.thickness)) return fail(G2_ERR_ARG, "giem2g_set_background: bad background");
+    op->Nl = bkg.Nl;
+    const double2 *cs = reinterpret_cast<const double2 *>(bkg.csigb);
+    op->csigma.assign(cs, cs + bkg.Nl + 1);
+    op->thick.clear();
+    if (bkg.Nl > 1) {
+        const double *th = reinterpret_cast<const double *>(bkg.thickness);
+        op->thick.assign(th, th + bkg.Nl - 1);
+    }
+    op->omega = omega;
+    // CREATE_BACKGROUND depth (giem2g_interfaces.F90:264-268), Lnumber (:163-165)
+    std::vector<double> depth(bkg.Nl + 1, 0.0);
+    if (bkg.Nl > 1) {
+        depth[1] = op->thick[0];
+        for (int i = 2; i <= bkg.Nl - 1; i++) depth[i] = depth[i - 1] + op->thick[i - 1];
+    }
+    const int Nz = op->Nz;
+    op->Lnumber.assign(Nz + 1, 0);
+    for (int i = 1; i <= Nz; i++) op->Lnumber[i] = get_layer((op->z[i - 1] + op->z[i]) / 2.0, bkg.Nl, depth);
+    op->Lnumber[0] = get_layer(op->z[0] * (1.0 - 1e-7), bkg.Nl, depth);
+    op->csigb.resize(Nz);
+    op->sqsigb.resize(Nz);
+    for (int iz = 1; iz <= Nz; iz++) {
+        const int l = op->Lnumber[iz];
+        if (l < 1) return fail(G2_ERR_ARG, "giem2g_set_background: anomaly cell %d is not below the surface", iz);
+        op->csigb[iz - 1] = op->csigma[l];
+        op->sqsigb[iz - 1] = std::sqrt(op->csigma[l].x);  // PreparePreconditioner (calc_ie_tensor_module.F90:303)
+    }
+    op->have_background = true;
+    if (op->have_sigma) {
+        int rc = ie_prepare_sigma(op, op->stream);
+        if (rc) return set_status(rc);
+    }
+    return set_status(0);
+}
+
+void giem2g_calc_ie_kernel(void *ie, GIEM2G_BACKGROUND_TYPE bkg, GIEM2G_ANOMALY_TYPE anomaly, double omega)
+{
+    IeOp *op = resolve(ie);
+    if (!op) { fail(G2_ERR_STATE, "giem2g_calc_ie_kernel: no operator"); return; }
+    if (anomaly.Nx != op->Nx || anomaly.Ny != op->Ny || anomaly.Nz != op->Nz) {
+        fail(G2_ERR_ARG, "giem2g_calc_ie_kernel: anomaly shape differs from the prepared operator");
+        return;
+    }
+    op->dx = anomaly.dx;
+    op->dy = anomaly.dy;
+    if (giem2g_set_background(op, bkg, omega)) return;
+    int rc = ie_green_tensor(op, op->stream);
+    if (rc) { fail(rc, "giem2g_calc_ie_kernel: %s", giem2g_last_error()); return; }
+    op->have_spatial = true;
+    op->have_spectral = false;
+    set_status(0);
+}
+
+int giem2g_set_ie_kernel_spatial(void *ie, const void *symm, const void *asym)
+{
+    IeOp *op = resolve(ie);
+    if (!op || op->z.empty()) return fail(G2_ERR_STATE, "giem2g_set_ie_kernel_spatial: operator not prepared");
+    const int P = op->P(), Nz = op->Nz, T = op->Tunit();
+    const size_t U = op->units();
+    if (!op->d_spatial && cudaMalloc(&op->d_spatial, U * T * sizeof(double2)) != cudaSuccess)
+        return fail(G2_ERR_NOMEM, "giem2g_set_ie_kernel_spatial: cudaMalloc failed");
+    std::vector<double2> h(U * T);
+    const double2 *s = reinterpret_cast<const double2 *>(symm), *a = reinterpret_cast<const double2 *>(asym);
+    for (size_t u = 0; u < U; u++) {
+        std::memcpy(&h[u * T], s + u * 4 * P, sizeof(double2) * 4 * P);
+        std::memcpy(&h[u * T + 4 * P], a + u * 2 * Nz * Nz, sizeof(double2) * 2 * Nz * Nz);
+    }
+    if (cudaMemcpy(op->d_spatial, h.data(), U * T * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(G2_ERR_CUDA, "giem2g_set_ie_kernel_spatial: copy failed");
+    op->have_spatial = true;
+    op->have_spectral = false;
+    return set_status(0);
+}
+
+static int get_units(IeOp *op, const double2 *d, void *symm, void *asym)
+{
+    const int P = op->P(), Nz = op->Nz, T = op->Tunit();
+    const size_t U = op->units();
+    std::vector<double2> h(U * T);
+    if (cudaMemcpy(h.data(), d, U * T * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(G2_ERR_CUDA, "tensor download failed");
+    double2 *s = reinterpret_cast<double2 *>(symm), *a = reinterpret_cast<double2 *>(asym);
+    for (size_t u = 0; u < U; u++) {
+        std::memcpy(s + u * 4 * P, &h[u * T], sizeof(double2) * 4 * P);
+        std::memcpy(a + u * 2 * Nz * Nz, &h[u * T + 4 * P], sizeof(double2) * 2 * Nz * Nz);
+    }
+    return set_status(0);
+}
+
+int giem2g_get_ie_kernel_spatial(void *ie, void *symm, void *asym)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !op->have_spatial) return fail(G2_ERR_STATE, "giem2g_get_ie_kernel_spatial: no spatial tensor");
+    return get_units(op, op->d_spatial, symm, asym);
+}
+
+int giem2g_get_ie_kernel_spectral(void *ie, void *symm, void *asym)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !op->have_spectral) return fail(G2_ERR_STATE, "giem2g_get_ie_kernel_spectral: no spectral tensor");
+    return get_units(op, op->d_tensor64, symm, asym);
+}
+
+void giem2g_calc_fft_of_ie_kernel(void *ie)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !op->have_spatial) { fail(G2_ERR_STATE, "giem2g_calc_fft_of_ie_kernel: no spatial tensor"); return; }
+    int rc = ie_tensor_spectrum(op, op->stream);
+    if (rc) { fail(rc, "giem2g_calc_fft_of_ie_kernel: %s", giem2g_last_error()); return; }
+    op->have_spectral = true;
+    set_status(0);
+}
+
+void giem2g_set_anomaly_conductivity(void *ie, void *csiga)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !op->d_csiga) { fail(G2_ERR_STATE, "giem2g_set_anomaly_conductivity: operator not prepared"); return; }
+    if (!csiga) { fail(G2_ERR_ARG, "giem2g_set_anomaly_conductivity: csiga is NULL"); return; }
+    if (cudaMemcpy(op->d_csiga, csiga, op->cells() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        fail(G2_ERR_CUDA, "giem2g_set_anomaly_conductivity: copy failed");
+        return;
+    }
+    op->have_sigma = true;
+    if (op->have_background) {
+        int rc = ie_prepare_sigma(op, op->stream);
+        if (rc) { fail(rc, "giem2g_set_anomaly_conductivity: %s", giem2g_last_error()); return; }
+    }
+    set_status(0);
+}
+
+static int check_ready(IeOp *op, const char *who)
+{
+    if (!op) return fail(G2_ERR_STATE, "%s: no operator", who);
+    if (!op->have_spectral) return fail(G2_ERR_STATE, "%s: spectral tensor missing (giem2g_calc_fft_of_ie_kernel)", who);
+    if (!op->have_sigma || !op->have_background) return fail(G2_ERR_STATE, "%s: conductivity/background missing", who);
+    return 0;
+}
+
+int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int precision)
+{
+    IeOp *op = resolve(ie);
+    int rc = check_ready(op, "giem2g_apply_ie_operator_device");
+    if (rc) return rc;
+    cudaEventRecord(op->ev0, op->stream);
+    if (precision == 0)
+        rc = ie_apply_device64(op, reinterpret_cast<const double2 *>(d_in), reinterpret_cast<double2 *>(d_out), op->stream);
+    else
+        rc = ie_apply_device32(op, reinterpret_cast<const float2 *>(d_in), reinterpret_cast<float2 *>(d_out), op->stream);
+    cudaEventRecord(op->ev1, op->stream);
+    op->last_kernel_launches = ie_kernel_launch_count_apply();
+    op->mult_num++;
+    if (rc) return fail(rc, "giem2g_apply_ie_operator_device: %s", giem2g_last_error());
+    return set_status(0);
+}
+
+void giem2g_apply_ie_operator(void *ie, void *in, void *out)
+{
+    // apply_ie_operator_module.F90:39 via giem2g_interfaces.F90:203-232: host vectors in/out
+    IeOp *op = resolve(ie);
+    if (check_ready(op, "giem2g_apply_ie_operator")) return;
+    const size_t nb = op->nvec() * sizeof(double2);
+    cudaMemcpyAsync(op->d_vin, in, nb, cudaMemcpyHostToDevice, op->stream);
+    int rc = giem2g_apply_ie_operator_device(op, op->d_vin, op->d_vout, 0);
+    if (rc) return;
+    cudaMemcpyAsync(out, op->d_vout, nb, cudaMemcpyDeviceToHost, op->stream);
+    if (cudaStreamSynchronize(op->stream) != cudaSuccess) { fail(G2_ERR_CUDA, "giem2g_apply_ie_operator: %s", cudaGetErrorString(cudaGetLastError())); return; }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, op->ev0, op->ev1);
+    op->apply_seconds += ms * 1e-3;
+    set_status(0);
+}
+
+void *giem2g_get_stream(void *ie)
+{
+    IeOp *op = resolve(ie);
+    return op ? (void *)op->stream : nullptr;
+}
+
+double giem2g_last_apply_ms(void *ie)
+{
+    IeOp *op = resolve(ie);
+    if (!op) return -1.0;
+    float ms = -1.0f;
+    if (cudaEventSynchronize(op->ev1) != cudaSuccess) return -1.0;
+    cudaEventElapsedTime(&ms, op->ev0, op->ev1);
+    return ms;
+}
+
+int giem2g_last_kernel_launches(void *ie)
+{
+    IeOp *op = resolve(ie);
+    return op ? op->last_kernel_launches : 0;
+}
+
+void giem2g_set_logger(void (*logger)(const char *)) { g_logger = logger; }
+
+void giem2g_print_stats(void *ie)
+{
+    // Integral_Equation_Module.F90:473-484 PRINT_STATS
+    IeOp *op = resolve(ie);
+    if (!op) return;
+    char buf[256];
+    g2_log("===================================================================================");
+    std::snprintf(buf, sizeof(buf), "Time for multiplications:                                 %12.5e s", op->apply_seconds);
+    g2_log(buf);
+    std::snprintf(buf, sizeof(buf), "Average mult:                                             %12.5e s",
+                  op->mult_num ? op->apply_seconds / op->mult_num : 0.0);
+    g2_log(buf);
+    std::snprintf(buf, sizeof(buf), "Number of matrix-vector multiplications:                  %12lld", op->mult_num);
+    g2_log(buf);
+    g2_log("===================================================================================");
+    op->mult_num = 0;
+    op->apply_seconds = 0;
+}
+
+void giem2g_delete_ie_operator(void *ie)
+{
+    IeOp *op = resolve(ie);
+    if (!op) return;
+    if (op->stream) cudaStreamSynchronize(op->stream);
+    krylov_free(op);
+    void *ptrs[] = {op->d_spatial, op->d_tensor64, op->d_tensor32, op->d_csiga, op->d_gsig64, op->d_asig64,
+                    op->d_gsig32, op->d_asig32, op->d_post64, op->d_post32, op->d_twx64, op->d_twy64,
+                    op->d_twx32, op->d_twy32, op->scratch.U1, op->scratch.Uhat, op->d_vin, op->d_vout};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (op->ev0) cudaEventDestroy(op->ev0);
+    if (op->ev1) cudaEventDestroy(op->ev1);
+    if (op->stream) cudaStreamDestroy(op->stream);
+    if (g_last_op == op) g_last_op = nullptr;
+    delete op;
+    set_status(0);
+}
+
+}  // extern "C"

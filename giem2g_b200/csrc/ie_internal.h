@@ -1,0 +1,79 @@
+// Internal state of one IE operator on one GPU, and the kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "../../include/giem2g.h"
+
+enum { G2_OK = 0, G2_ERR_ARG = -1, G2_ERR_CUDA = -2, G2_ERR_STATE = -3, G2_ERR_UNSUPPORTED = -4,
+       G2_ERR_NUMERIC = -5, G2_ERR_NOMEM = -6 };
+
+struct ApplyScratch {
+    void *U1 = nullptr;    // [2Nx][3Nz][Ny]   x-spectrum / inverse-y output
+    void *Uhat = nullptr;  // [Nx][Ny][4][3Nz] full 2-D spectrum in (kx-pair, ky-pair, slot) order
+};
+
+struct IeOp {
+    // geometry
+    int Nx = 0, Ny = 0, Nz = 0;
+    double dx = 0, dy = 0;
+    std::vector<double> z, dz;
+    // background (complex conductivity per layer, index 0 = air)
+    int Nl = 0;
+    std::vector<double2> csigma;
+    std::vector<double> thick;
+    double omega = 0;
+    std::vector<int> Lnumber;          // 0..Nz
+    std::vector<double2> csigb;        // per cell layer
+    std::vector<double> sqsigb;
+    bool have_background = false;
+    bool have_spatial = false, have_spectral = false, have_sigma = false;
+    // device data
+    double2 *d_spatial = nullptr;      // [Nx][Ny][Tunit] FP64 spatial tensor
+    double2 *d_tensor64 = nullptr;     // [Nx][Ny][Tunit] FP64 spectral tensor
+    float2 *d_tensor32 = nullptr;      // same, complex64 copy
+    double2 *d_csiga = nullptr;        // [Nz][Ny][Nx]
+    double2 *d_gsig64 = nullptr, *d_asig64 = nullptr;  // per-cell pre/post coefficients
+    float2 *d_gsig32 = nullptr, *d_asig32 = nullptr;
+    double *d_post64 = nullptr;        // [2][Nz]: sqrt(Re sigma_b), 1/(dz*4NxNy)
+    float *d_post32 = nullptr;
+    double2 *d_twx64 = nullptr, *d_twy64 = nullptr;
+    float2 *d_twx32 = nullptr, *d_twy32 = nullptr;
+    ApplyScratch scratch;
+    // host staging for the reference-facing (host-pointer) apply
+    double2 *h_stage_in = nullptr, *h_stage_out = nullptr;
+    double2 *d_vin = nullptr, *d_vout = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
+    // counters (Integral_Equation_Module.F90:44-56)
+    long long mult_num = 0;
+    double apply_seconds = 0;
+    int last_kernel_launches = 0;
+
+    int P() const { return Nz * (Nz + 1) / 2; }
+    int Tunit() const { return 4 * P() + 2 * Nz * Nz; }
+    size_t units() const { return (size_t)Nx * Ny; }
+    size_t cells() const { return (size_t)Nx * Ny * Nz; }
+    size_t nvec() const { return 3 * cells(); }
+};
+
+// apply.cu
+int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st);
+int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st);
+int ie_alloc_scratch(IeOp *op);
+int ie_make_twiddles(IeOp *op);
+int ie_kernel_launch_count_apply();
+
+// green.cu: spatial Green's tensor (FP64) into op->d_spatial
+int ie_green_tensor(IeOp *op, cudaStream_t st);
+
+// tensor_fft.cu
+int ie_tensor_spectrum(IeOp *op, cudaStream_t st);
+
+// sigma.cu (in apply.cu)
+int ie_prepare_sigma(IeOp *op, cudaStream_t st);
+
+void g2_log(const char *msg);
+void g2_set_error(const char *file, int line, const char *msg);
+void g2_set_error_msg(const std::string &msg);

@@ -1,0 +1,137 @@
+/*
+ * giem2g.h -- C ABI of the B200 implementation of GIEM2G's integral-equation solve path.
+ *
+ * The first block re-exports the nine BIND(C) entry points of the reference's
+ * C interface with identical names, argument lists and struct layouts, so a host
+ * that links the reference's libgiem2g can link this library instead.  Citations
+ * are to giem2g_interfaces.F90 in the GIEM2G source tree.
+ *
+ * Differences from the reference that a caller can observe:
+ *   - One process drives one GPU; the communicator in GIEM2G_DATA_TYPE.comm64 is
+ *     ignored and every array covers the whole anomaly (Ny_loc == Ny).
+ *   - The caller-allocated kernel/FFT buffers named in GIEM2G_DATA_TYPE are not
+ *     used (their sizes are still reported); the tensor and spectra live on the GPU.
+ *   - giem2g_set_anomaly_conductivity copies csiga to the GPU at call time (the
+ *     reference keeps a pointer to the caller's array and re-reads it on every
+ *     apply); call it again after changing csiga.
+ *   - Errors are recorded: giem2g_last_status() returns 0 or a negative code and
+ *     giem2g_last_error() the message.  The reference has no error return.
+ *   - Nx and Ny must be even with 2*Nx and 2*Ny powers of two (4..1024).
+ *
+ * Vectors are complex(8) (Nx,Ny,Nz,3), x fastest, components (Ex,Ey,Ez).
+ */
+#ifndef GIEM2G_H
+#define GIEM2G_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* giem2g_interfaces.F90:33-37 */
+typedef struct {
+    int Nl;              /* number of layers (half-space included) */
+    void *csigb;         /* Nl+1 complex(8): [0] = air, then layers */
+    void *thickness;     /* Nl-1 real(8) */
+} GIEM2G_BACKGROUND_TYPE;
+
+/* giem2g_interfaces.F90:39-44 */
+typedef struct {
+    int Nx, Ny, Nz;
+    double dx, dy;
+    void *z;             /* Nz+1 real(8) cell borders */
+    void *dz;            /* Nz real(8) cell thicknesses */
+} GIEM2G_ANOMALY_TYPE;
+
+/* giem2g_interfaces.F90:46-58 */
+typedef struct {
+    long long tensor_size;
+    long long ie_kernel_buffer_length;
+    long long fft_buffers_length;
+    long long comm64;
+    void *giem2g_tensor;  /* out of giem2g_calc_data_sizes: the operator handle */
+    void *dz;
+    void *sqsigb;
+    void *csigb;
+    void *kernel_buffer;
+    void *fft_buffer_in;
+    void *fft_buffer_out;
+} GIEM2G_DATA_TYPE;
+
+/* ---- reference entry points --------------------------------------------- */
+/* giem2g_interfaces.F90:76-100  sizes + allocation of the operator handle */
+void giem2g_calc_data_sizes(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE *data);
+/* giem2g_interfaces.F90:102-141 geometry, device buffers */
+void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data);
+/* giem2g_interfaces.F90:144-174 spatial Green's tensor for angular frequency omega (FP64, GPU) */
+void giem2g_calc_ie_kernel(void *ie, GIEM2G_BACKGROUND_TYPE bkg, GIEM2G_ANOMALY_TYPE anomaly, double omega);
+/* giem2g_interfaces.F90:176-188 spectral transform of the tensor (FP64, GPU) */
+void giem2g_calc_fft_of_ie_kernel(void *ie);
+/* giem2g_interfaces.F90:190-201 csiga: Nx*Ny*Nz complex(8), x fastest */
+void giem2g_set_anomaly_conductivity(void *ie, void *csiga);
+/* giem2g_interfaces.F90:203-232 out = A in, host arrays of 3*Nx*Ny*Nz complex(8) */
+void giem2g_apply_ie_operator(void *ie, void *in, void *out);
+/* giem2g_interfaces.F90:234-238 */
+void giem2g_set_logger(void (*logger)(const char *));
+/* giem2g_interfaces.F90:240-247 */
+void giem2g_print_stats(void *ie);
+/* giem2g_interfaces.F90:248-254 (this implementation also frees the handle) */
+void giem2g_delete_ie_operator(void *ie);
+
+/* ---- status ---------------------------------------------------------------- */
+int giem2g_last_status(void);
+const char *giem2g_last_error(void);
+
+/* ---- extensions -------------------------------------------------------------- */
+/* Background only (PreparePreconditioner, calc_ie_tensor_module.F90:295-306):
+ * layer numbers, per-cell csigb and sqrt(Re csigb), without computing the tensor. */
+int giem2g_set_background(void *ie, GIEM2G_BACKGROUND_TYPE bkg, double omega);
+/* Upload / download the FP64 spatial tensor.  symm: [Nx][Ny][4][Nz(Nz+1)/2] packed upper
+ * (xx,xy,yy,zz), asym: [Nx][Ny][2][Nz*Nz] column-major (xz,yz) -- the reference's
+ * G_symm / G_asym of calc_ie_tensor_module.F90:278-288 with all ly on one process. */
+int giem2g_set_ie_kernel_spatial(void *ie, const void *symm, const void *asym);
+int giem2g_get_ie_kernel_spatial(void *ie, void *symm, void *asym);
+/* Download the spectral tensor in the same shapes, indexed [kx-pair][ky] (G_symmT/G_asymT). */
+int giem2g_get_ie_kernel_spectral(void *ie, void *symm_hat, void *asym_hat);
+/* Device-pointer apply on the operator's stream.  precision 0: complex128 vectors and
+ * FP64 tensor; precision 1: complex64 vectors and tensor (FP32 accumulation). */
+int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int precision);
+/* CUDA stream the operator's kernels run on (cudaStream_t). */
+void *giem2g_get_stream(void *ie);
+/* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */
+double giem2g_last_apply_ms(void *ie);
+int giem2g_last_kernel_launches(void *ie);
+
+/* FGMRES_CTL_TYPE (data_types_module.F90:49-55) */
+typedef struct {
+    double misfit;       /* outer tolerance */
+    int fgmres_maxit;    /* MaxRestart */
+    int gmres_buf;       /* InnerBufferSize */
+    int fgmres_buf;      /* OuterBufferSize */
+    int precision;       /* 0 plain FP64; 1 mixed: complex64 inner GMRES, FP64 outer */
+} GIEM2G_FGMRES_CTL;
+
+/* RESULT_INFO (GFGMRES/fgmres_interfaces.F90:34-39) + counters */
+typedef struct {
+    int iterations;
+    double bea;          /* Arnoldi misfit */
+    double be;           /* true misfit */
+    int stat;            /* 1 CONVERGED, 2 NON_TRUE_CONVERGED, -1 NON_CONVERGED, -3 INTERUPTED */
+    int applies_fp64;
+    int applies_fp32;
+    double device_ms;
+} GIEM2G_RESULT;
+
+/* SolveEquation (ie_solver_module.F90:43-114): E_bkg, Esol, E0 host arrays (Nx,Ny,Nz,3)
+ * complex(8); E0 may be NULL (guess = sqrt(Re sigma_b) * E_bkg).  Esol receives a*chi. */
+int giem2g_solve(void *ie, const void *E_bkg, void *Esol, const void *E0, GIEM2G_FGMRES_CTL ctl,
+                 GIEM2G_RESULT *info);
+/* Same with device pointers (complex128), on the operator's stream. */
+int giem2g_solve_device(void *ie, const void *d_E_bkg, void *d_Esol, const void *d_E0, GIEM2G_FGMRES_CTL ctl,
+                        GIEM2G_RESULT *info);
+/* Outer Arnoldi misfit after each outer iteration of the last solve; returns the count copied. */
+int giem2g_get_misfit_history(void *ie, double *out, int max_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
