@@ -67,7 +67,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_last_status", "giem2g_last_error", "giem2g_set_background", "giem2g_set_ie_kernel_spatial",
     "giem2g_get_ie_kernel_spatial", "giem2g_get_ie_kernel_spectral", "giem2g_apply_ie_operator_device",
     "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_solve",
-    "giem2g_solve_device", "giem2g_get_misfit_history",
+    "giem2g_solve_device", "giem2g_get_misfit_history", "giem2g_check_device_error",
 ]
 
 
@@ -115,6 +115,7 @@ def lib():
     L.giem2g_solve.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
     L.giem2g_solve_device.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
     L.giem2g_get_misfit_history.argtypes = [vp, vp, ip]
+    L.giem2g_check_device_error.argtypes = [vp]
     _lib = L
     return L
 
@@ -231,6 +232,9 @@ class IEOperator:
 
     def apply_device(self, d_in: int, d_out: int, precision: int = 0):
         _check(lib().giem2g_apply_ie_operator_device(self.handle, d_in, d_out, precision), "apply_device")
+
+    def check_device_error(self):
+        _check(lib().giem2g_check_device_error(self.handle), "device error word")
 
     @property
     def stream(self) -> int:

@@ -317,7 +317,17 @@ static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream
         k_fwd_y<R><<<grid, kThreads, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, TC);
     }
     // contraction
-    {
+    int rc_fast = G2_ERR_UNSUPPORTED;
+    if (op->use_fast_contract) {
+        if (sizeof(R) == 8)
+            rc_fast = ie_contract_fast64(reinterpret_cast<const double2 *>(G), reinterpret_cast<double2 *>(Uh), Nx, Ny,
+                                         Nz, op->d_err, st);
+        else
+            rc_fast = ie_contract_fast32(reinterpret_cast<const float2 *>(G), reinterpret_cast<float2 *>(Uh), Nx, Ny,
+                                         Nz, op->d_err, st);
+        if (rc_fast != G2_OK && rc_fast != G2_ERR_UNSUPPORTED) return rc_fast;
+    }
+    if (rc_fast != G2_OK) {
         const int T = op->Tunit();
         const size_t sm = ((size_t)T + 4 * Z3) * es;
         const int threads = ((Z3 + 31) / 32) * 32;

@@ -1,6 +1,7 @@
 // C ABI: the reference's giem2g_* entry points (giem2g_interfaces.F90:76-254) plus extensions.
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -129,8 +130,16 @@ void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data
     }
     cudaEventCreate(&op->ev0);
     cudaEventCreate(&op->ev1);
+    {
+        const char *gen = std::getenv("GIEM2G_GENERIC_CONTRACT");
+        op->use_fast_contract = !(gen && gen[0] == '1');
+    }
     int rc = ie_make_twiddles(op);
     if (!rc) rc = ie_alloc_scratch(op);
+    if (!rc && !op->d_err) {
+        if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
+            rc = G2_ERR_NOMEM;
+    }
     if (!rc && !op->d_csiga && cudaMalloc(&op->d_csiga, op->cells() * sizeof(double2)) != cudaSuccess) rc = G2_ERR_NOMEM;
     if (!rc && !op->d_vin) {
         if (cudaMalloc(&op->d_vin, op->nvec() * sizeof(double2)) != cudaSuccess ||
@@ -313,10 +322,20 @@ void giem2g_apply_ie_operator(void *ie, void *in, void *out)
     if (rc) return;
     cudaMemcpyAsync(out, op->d_vout, nb, cudaMemcpyDeviceToHost, op->stream);
     if (cudaStreamSynchronize(op->stream) != cudaSuccess) { fail(G2_ERR_CUDA, "giem2g_apply_ie_operator: %s", cudaGetErrorString(cudaGetLastError())); return; }
+    if (ie_check_device_error(op)) return;
     float ms = 0;
     cudaEventElapsedTime(&ms, op->ev0, op->ev1);
     op->apply_seconds += ms * 1e-3;
     set_status(0);
+}
+
+int giem2g_check_device_error(void *ie)
+{
+    IeOp *op = resolve(ie);
+    if (!op) return fail(G2_ERR_STATE, "giem2g_check_device_error: no operator");
+    if (cudaStreamSynchronize(op->stream) != cudaSuccess) return fail(G2_ERR_CUDA, "%s", cudaGetErrorString(cudaGetLastError()));
+    int rc = ie_check_device_error(op);
+    return rc ? rc : set_status(0);
 }
 
 void *giem2g_get_stream(void *ie)
@@ -370,7 +389,7 @@ void giem2g_delete_ie_operator(void *ie)
     krylov_free(op);
     void *ptrs[] = {op->d_spatial, op->d_tensor64, op->d_tensor32, op->d_csiga, op->d_gsig64, op->d_asig64,
                     op->d_gsig32, op->d_asig32, op->d_post64, op->d_post32, op->d_twx64, op->d_twy64,
-                    op->d_twx32, op->d_twy32, op->scratch.U1, op->scratch.Uhat, op->d_vin, op->d_vout};
+                    op->d_twx32, op->d_twy32, op->scratch.U1, op->scratch.Uhat, op->d_vin, op->d_vout, op->d_err};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (op->ev0) cudaEventDestroy(op->ev0);
@@ -382,3 +401,16 @@ void giem2g_delete_ie_operator(void *ie)
 }
 
 }  // extern "C"
+
+int ie_check_device_error(IeOp *op)
+{
+    int h = 0;
+    if (!op->d_err) return 0;
+    if (cudaMemcpy(&h, op->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(G2_ERR_CUDA, "error-word read failed");
+    if (h) {
+        cudaMemset(op->d_err, 0, sizeof(int));
+        return fail(G2_ERR_NUMERIC, "device wait limit reached (code %d)", h);
+    }
+    return 0;
+}

@@ -40,12 +40,14 @@ struct IeOp {
     double2 *d_twx64 = nullptr, *d_twy64 = nullptr;
     float2 *d_twx32 = nullptr, *d_twy32 = nullptr;
     ApplyScratch scratch;
+    int *d_err = nullptr;              // device error word written by bounded waits (0 = ok)
     // host staging for the reference-facing (host-pointer) apply
     double2 *h_stage_in = nullptr, *h_stage_out = nullptr;
     double2 *d_vin = nullptr, *d_vout = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
+    bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
     // counters (Integral_Equation_Module.F90:44-56)
     long long mult_num = 0;
     double apply_seconds = 0;
@@ -68,12 +70,17 @@ int ie_kernel_launch_count_apply();
 // green.cu: spatial Green's tensor (FP64) into op->d_spatial
 int ie_green_tensor(IeOp *op, cudaStream_t st);
 
+// contract.cu: specialised contraction; G2_ERR_UNSUPPORTED when Nz has no specialisation
+int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st);
+int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st);
+
 // tensor_fft.cu
 int ie_tensor_spectrum(IeOp *op, cudaStream_t st);
 
 // sigma.cu (in apply.cu)
 int ie_prepare_sigma(IeOp *op, cudaStream_t st);
 
+int ie_check_device_error(IeOp *op);  // reads d_err after a sync; nonzero -> G2_ERR_NUMERIC
 void g2_log(const char *msg);
 void g2_set_error(const char *file, int line, const char *msg);
 void g2_set_error_msg(const std::string &msg);

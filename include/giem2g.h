@@ -95,6 +95,9 @@ int giem2g_get_ie_kernel_spectral(void *ie, void *symm_hat, void *asym_hat);
 /* Device-pointer apply on the operator's stream.  precision 0: complex128 vectors and
  * FP64 tensor; precision 1: complex64 vectors and tensor (FP32 accumulation). */
 int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int precision);
+/* Synchronise the operator's stream and report a device-side error word (bounded waits that ran
+ * out) as a nonzero status. */
+int giem2g_check_device_error(void *ie);
 /* CUDA stream the operator's kernels run on (cudaStream_t). */
 void *giem2g_get_stream(void *ie);
 /* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */

@@ -25,6 +25,13 @@ def random_spatial_tensor(m, seed=3, scale=1.0):
     P = m.Nz * (m.Nz + 1) // 2
     s = (rng.standard_normal((m.Nx, m.Ny, 4, P)) + 1j * rng.standard_normal((m.Nx, m.Ny, 4, P))) * scale
     a = (rng.standard_normal((m.Nx, m.Ny, 2, m.Nz * m.Nz)) + 1j * rng.standard_normal((m.Nx, m.Ny, 2, m.Nz * m.Nz))) * scale
+    # components odd in a direction vanish at lag 0 of that direction (xy: x and y, xz: x, yz: y),
+    # as the physical tensor does (calc_ie_tensor_module.F90:328-350 zero those weights); the
+    # spectral pairing of the reference relies on it
+    s[0, :, 1] = 0
+    s[:, 0, 1] = 0
+    a[0, :, 0] = 0
+    a[:, 0, 1] = 0
     return s, a
 
 

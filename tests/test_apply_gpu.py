@@ -26,7 +26,8 @@ def _setup(g2, orc, m, symm, asym, sig):
     return op, csiga, csigb, sqsigb
 
 
-@pytest.mark.parametrize("shape", [(2, 2, 1), (4, 4, 3), (8, 4, 5), (4, 16, 2), (16, 8, 7)])
+@pytest.mark.parametrize("shape", [(2, 2, 1), (4, 4, 3), (8, 4, 5), (4, 16, 2), (16, 8, 7), (4, 4, 8), (8, 4, 16),
+                                   (4, 4, 32), (2, 4, 48)])
 def test_spectrum_and_apply_random_tensor(g2lib, orc, shape):
     m = tiny_model(*shape)
     symm, asym = random_spatial_tensor(m)
@@ -79,3 +80,31 @@ def test_apply_complex64_device(g2lib, orc):
     assert rel(do64.cpu().numpy().reshape(v.shape), out_o) < TOL64
     assert op.last_kernel_launches() == 5
     op.delete()
+
+
+@pytest.mark.parametrize("shape", [(4, 4, 8), (8, 4, 16), (4, 4, 32), (2, 4, 48)])
+def test_complex64_specialised_and_generic_contraction(g2lib, orc, shape, monkeypatch):
+    """complex64 path for the specialised Nz kernels and the generic kernel give the oracle's result."""
+    import torch
+    m = tiny_model(*shape)
+    symm, asym = random_spatial_tensor(m)
+    sig = random_sigma(m)
+    sh_o, ah_o = orc.tensor_spectrum(m.Nx, m.Ny, m.Nz, symm, asym)
+    csigb, sqsigb = orc.background_cells(m)
+    v = random_vec(m, 9)
+    csiga = csiga_from_sigma(sig, m.freq)
+    out_o = orc.apply(m.Nx, m.Ny, m.Nz, sh_o, ah_o, csiga, csigb, sqsigb, m.dz, v)
+    for generic in ("0", "1"):
+        monkeypatch.setenv("GIEM2G_GENERIC_CONTRACT", generic)
+        op, *_ = _setup(g2lib, orc, m, symm, asym, sig)
+        dv = torch.from_numpy(v.astype(np.complex64).ravel()).cuda()
+        do = torch.empty_like(dv)
+        op.apply_device(dv.data_ptr(), do.data_ptr(), precision=1)
+        op.check_device_error()
+        assert rel(do.cpu().numpy().reshape(v.shape), out_o) < TOL32
+        dv64 = torch.from_numpy(v.ravel()).cuda()
+        do64 = torch.empty_like(dv64)
+        op.apply_device(dv64.data_ptr(), do64.data_ptr(), precision=0)
+        op.check_device_error()
+        assert rel(do64.cpu().numpy().reshape(v.shape), out_o) < TOL64
+        op.delete()
