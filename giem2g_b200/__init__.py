@@ -68,6 +68,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_get_ie_kernel_spatial", "giem2g_get_ie_kernel_spectral", "giem2g_apply_ie_operator_device",
     "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_solve",
     "giem2g_solve_device", "giem2g_get_misfit_history", "giem2g_check_device_error",
+    "giem2g_contract_variants", "giem2g_set_contract_variant",
 ]
 
 
@@ -116,6 +117,8 @@ def lib():
     L.giem2g_solve_device.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
     L.giem2g_get_misfit_history.argtypes = [vp, vp, ip]
     L.giem2g_check_device_error.argtypes = [vp]
+    L.giem2g_contract_variants.argtypes = [vp, ip]
+    L.giem2g_set_contract_variant.argtypes = [vp, ip, ip]
     _lib = L
     return L
 
@@ -232,6 +235,12 @@ class IEOperator:
 
     def apply_device(self, d_in: int, d_out: int, precision: int = 0):
         _check(lib().giem2g_apply_ie_operator_device(self.handle, d_in, d_out, precision), "apply_device")
+
+    def contract_variants(self, precision: int) -> int:
+        return lib().giem2g_contract_variants(self.handle, precision)
+
+    def set_contract_variant(self, precision: int, variant: int):
+        _check(lib().giem2g_set_contract_variant(self.handle, precision, variant), "set_contract_variant")
 
     def check_device_error(self):
         _check(lib().giem2g_check_device_error(self.handle), "device error word")

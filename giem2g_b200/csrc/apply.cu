@@ -3,16 +3,20 @@
 // Restates APPLY_PRECOND / MULT_IE_OP (apply_ie_operator_module.F90:39-263) without the MPI
 // slab decomposition: the padded 2Nx x 2Ny transform of the reference's Distributed_FFT.F90
 // becomes five kernels over HBM-resident buffers:
-//   k_fwd_x    pre-scale by gsig, zero-pad in x, forward x-FFT          x   -> U1[kx][zc][y]
-//   k_fwd_y    zero-pad in y, forward y-FFT, scatter to (q,r,slot)      U1  -> Uhat[q][r][4][zc]
-//   k_contract per (q,r): 6 Green's blocks applied to the 4 points (+-kx,+-ky)   Uhat in place
-//   k_bwd_y    inverse y-FFT, crop y<Ny                                 Uhat -> U1
-//   k_bwd_x    inverse x-FFT, crop x<Nx, post-combine                   U1  -> y
+//   k_fx       pre-scale by gsig, zero-pad in x, forward x-FFT          x   -> U1[kx][y][zc]
+//   k_fy       zero-pad in y, forward y-FFT, scatter to (q,r,slot)      U1  -> Uhat[q][r][4][zc]
+//   contraction per (q,r): 6 Green's blocks applied to the 4 points (+-kx,+-ky)   Uhat in place
+//              (contract.cu, TMA-pipelined; k_contract below is the generic fallback)
+//   k_by       inverse y-FFT, crop y<Ny                                 Uhat -> U1
+//   k_bx       inverse x-FFT, crop x<Nx, post-combine                   U1  -> y
+// The transforms are four-step register FFTs (fft4.cuh) with one shared-memory transpose; zc = c*Nz+z
+// is the fastest index of the intermediates so every global access is coalesced.
 // (kx-pair q, ky-pair r, slot s) <-> (kx,ky): kx = q (s&2==0) or 2Nx-q, with q=0,s&2 the x-Nyquist;
 // ky = r (s&1==0) or 2Ny-r, with r=0,s&1 the y-Nyquist.  Nyquist outputs are zero as in the
 // reference (FinalTransposeRepack / DistributedFourierYRepack drop them).
 #include <type_traits>
 #include "common.cuh"
+#include "fft4.cuh"
 #include "ie_internal.h"
 
 namespace {
@@ -21,38 +25,7 @@ template <typename R> using CT = typename Cplx<R>::T;
 
 constexpr int kThreads = 256;
 
-// ---------------------------------------------------------------------------------------------
-// k_fwd_x: one CTA = TY consecutive y rows of one (z,c) line set.  apply_ie_operator_module.F90:57-115
-template <typename R>
-__global__ void __launch_bounds__(kThreads) k_fwd_x(const CT<R> *__restrict__ vin, const CT<R> *__restrict__ gsig,
-                                                    CT<R> *__restrict__ U1, const CT<R> *__restrict__ tw, int Nx,
-                                                    int Ny, int Nz, int TY)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
-    const int L = 2 * Nx, lg = ilog2(L), ls = L + 1;
-    const int y0 = blockIdx.x * TY, zc = blockIdx.y, z = zc % Nz;
-    const int nl = min(TY, Ny - y0);
-    const size_t plane = (size_t)Nx * Ny;
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-        const int t = i / L, x = i - t * L;
-        CT<R> v = czero<CT<R>>();
-        if (x < Nx) {
-            const size_t cell = (size_t)z * plane + (size_t)(y0 + t) * Nx + x;
-            v = cmul(vin[(size_t)zc * plane + (size_t)(y0 + t) * Nx + x], gsig[cell]);
-        }
-        s[t * ls + bitrev(x, lg)] = v;
-    }
-    __syncthreads();
-    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, false);
-    const int Z3 = 3 * Nz;
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-        const int kx = i / nl, t = i - kx * nl;
-        U1[((size_t)kx * Z3 + zc) * Ny + y0 + t] = s[t * ls + kx];
-    }
-}
-
-// slot helpers
+// slot helpers: (kx-pair q, slot bit) and (ky-pair r, mirror bit) of a spectral index
 G2_D void kx_to_slot(int kx, int Nx, int &q, int &sx)
 {
     if (kx < Nx) { q = kx; sx = 0; }
@@ -66,42 +39,136 @@ G2_D void ky_to_slot(int ky, int Ny, int &r, int &sy)
     else { r = 2 * Ny - ky; sy = 1; }
 }
 
-// ---------------------------------------------------------------------------------------------
-// k_fwd_y: one CTA = one kx column x TC (z,c) lines.  Distributed_FFT.F90:437-505 (y part + repack)
-template <typename R>
-__global__ void __launch_bounds__(kThreads) k_fwd_y(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uhat,
-                                                    const CT<R> *__restrict__ tw, int Nx, int Ny, int Nz, int TC)
+template <typename C>
+G2_D void load_tw(C *dst, const C *__restrict__ src, int L)
 {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_fx: pre-scale by gsig, zero-pad to 2Nx, forward x-FFT.  CTA = one y row x NL (z,c) lines.
+// apply_ie_operator_module.F90:57-115 + Distributed_FFT.F90:552-569
+template <typename R, int L>
+__global__ void __launch_bounds__(kThreads) k_fx(const CT<R> *__restrict__ vin, const CT<R> *__restrict__ gsig,
+                                                 CT<R> *__restrict__ U1, const CT<R> *__restrict__ twg, int Nx,
+                                                 int Ny, int Nz, int NL)
+{
+    using C = CT<R>;
+    constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
-    const int L = 2 * Ny, lg = ilog2(L), ls = L + 1, Z3 = 3 * Nz;
-    const int kx = blockIdx.x, zc0 = blockIdx.y * TC;
-    const int nl = min(TC, Z3 - zc0);
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *sm = tw + L;
+    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, y = blockIdx.y;
+    const int nl = min(NL, Z3 - zc0);
+    const size_t plane = (size_t)Nx * Ny;
+    load_tw(tw, twg, L);
+    __syncthreads();
+    auto load = [&](int t, int x) -> C {
+        const int zc = zc0 + t, z = zc % Nz;
+        return cmul(vin[(size_t)zc * plane + (size_t)y * Nx + x], gsig[(size_t)z * plane + (size_t)y * Nx + x]);
+    };
+    auto store = [&](int t, int kx, C v) { U1[((size_t)kx * Ny + y) * Z3 + zc0 + t] = v; };
+    auto off = [&](int t, int n1, int k2) { return n1 + N1 * k2 + (L + 1) * t; };
+    fft4step<C, N1, N2, false, true, false, false, true>(sm, nl, tw, load, store, off);
+}
+
+// k_fy: zero-pad to 2Ny, forward y-FFT of one kx column, scatter to (q, r, slot).
+// Distributed_FFT.F90:437-505 (y transform + +-ky repack) and :639-694 (+-kx repack)
+template <typename R, int L>
+__global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uh,
+                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL)
+{
+    using C = CT<R>;
+    constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *sm = tw + L;
+    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, kx = blockIdx.y;
+    const int nl = min(NL, Z3 - zc0);
     int q, sx;
     kx_to_slot(kx, Nx, q, sx);
-    if (kx == Nx) {  // x-Nyquist column: never used, keep it zero
+    if (kx == Nx) {  // x-Nyquist column: kept zero
         for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-            const int ky = i / nl, t = i - ky * nl;
+            const int t = i % nl, ky = i / nl;
             int r, sy;
             ky_to_slot(ky, Ny, r, sy);
-            Uhat[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = czero<CT<R>>();
+            Uh[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = czero<C>();
         }
         return;
     }
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-        const int t = i / L, y = i - t * L;
-        CT<R> v = czero<CT<R>>();
-        if (y < Ny) v = U1[((size_t)kx * Z3 + zc0 + t) * Ny + y];
-        s[t * ls + bitrev(y, lg)] = v;
-    }
+    load_tw(tw, twg, L);
     __syncthreads();
-    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, false);
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-        const int ky = i / nl, t = i - ky * nl;
+    auto load = [&](int t, int yy) -> C { return U1[((size_t)kx * Ny + yy) * Z3 + zc0 + t]; };
+    auto store = [&](int t, int ky, C v) {
         int r, sy;
         ky_to_slot(ky, Ny, r, sy);
-        Uhat[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = s[t * ls + ky];
-    }
+        Uh[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = v;
+    };
+    auto off = [&](int t, int n1, int k2) { return t + NL * (n1 + N1 * k2); };
+    fft4step<C, N1, N2, false, true, false, true, true>(sm, nl, tw, load, store, off);
+}
+
+// k_by: inverse y-FFT of one kx column, crop y < Ny.  Distributed_FFT.F90:455-476, 696-788
+template <typename R, int L>
+__global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, CT<R> *__restrict__ U1,
+                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL)
+{
+    using C = CT<R>;
+    constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *sm = tw + L;
+    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, kx = blockIdx.y;
+    if (kx == Nx) return;  // x-Nyquist column is read as zero by k_bx
+    const int nl = min(NL, Z3 - zc0);
+    int q, sx;
+    kx_to_slot(kx, Nx, q, sx);
+    load_tw(tw, twg, L);
+    __syncthreads();
+    auto load = [&](int t, int ky) -> C {
+        int r, sy;
+        ky_to_slot(ky, Ny, r, sy);
+        return Uh[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t];
+    };
+    auto store = [&](int t, int yy, C v) { U1[((size_t)kx * Ny + yy) * Z3 + zc0 + t] = v; };
+    auto off = [&](int t, int n1, int k2) { return t + NL * (n1 + N1 * k2); };
+    fft4step<C, N1, N2, true, false, true, true, true>(sm, nl, tw, load, store, off);
+}
+
+// k_bx: inverse x-FFT, crop x < Nx, post-combine y = s*(a*x - w/(dz*4NxNy)).
+// apply_ie_operator_module.F90:125-174
+template <typename R, int L>
+__global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, const CT<R> *__restrict__ vin,
+                                                 const CT<R> *__restrict__ asig, const R *__restrict__ post,
+                                                 CT<R> *__restrict__ vout, const CT<R> *__restrict__ twg, int Nx,
+                                                 int Ny, int Nz, int NL)
+{
+    using C = CT<R>;
+    constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw = reinterpret_cast<C *>(smem_raw);
+    C *sm = tw + L;
+    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, y = blockIdx.y;
+    const int nl = min(NL, Z3 - zc0);
+    const size_t plane = (size_t)Nx * Ny;
+    load_tw(tw, twg, L);
+    __syncthreads();
+    auto load = [&](int t, int kx) -> C {
+        return kx == Nx ? czero<C>() : U1[((size_t)kx * Ny + y) * Z3 + zc0 + t];
+    };
+    auto store = [&](int t, int x, C w) {
+        const int zc = zc0 + t, z = zc % Nz;
+        const size_t cell = (size_t)z * plane + (size_t)y * Nx + x;
+        const size_t idx = (size_t)zc * plane + (size_t)y * Nx + x;
+        const C d1 = cmul(vin[idx], asig[cell]);
+        const R sq = post[z], inv = post[Nz + z];
+        C o;
+        o.x = (d1.x - w.x * inv) * sq;
+        o.y = (d1.y - w.y * inv) * sq;
+        vout[idx] = o;
+    };
+    auto off = [&](int t, int n1, int k2) { return t * (L + 1) + k2 + N2 * n1; };
+    fft4step<C, N1, N2, true, false, true, true, false>(sm, nl, tw, load, store, off);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -113,6 +180,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_y(const CT<R> *__restrict__ U1
 template <typename R>
 __global__ void k_contract(const CT<R> *__restrict__ G, CT<R> *__restrict__ Uhat, int Nx, int Ny, int Nz)
 {
+    const int AW = sizeof(R) == 8 ? asw_width64(Nz) : asw_width32(Nz);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = Nz * (Nz + 1) / 2, T = 4 * P + 2 * Nz * Nz, Z3 = 3 * Nz;
     CT<R> *sg = reinterpret_cast<CT<R> *>(smem_raw);
@@ -154,8 +222,8 @@ __global__ void k_contract(const CT<R> *__restrict__ G, CT<R> *__restrict__ Uhat
         for (int zp = 0; zp < Nz; zp++) {
             CT<R> g;
             if (kind == 0) g = (z <= zp) ? blk[z + zp * (zp + 1) / 2] : blk[zp + z * (z + 1) / 2];
-            else if (kind == 1) g = blk[z + zp * Nz];
-            else g = blk[zp + z * Nz];
+            else if (kind == 1) g = blk[asw(z, zp, Nz, AW)];
+            else g = blk[asw(zp, z, Nz, AW)];
 #pragma unroll
             for (int p = 0; p < 4; p++) cfma(part[p], g, u[p * Z3 + zp]);
         }
@@ -177,70 +245,6 @@ __global__ void k_contract(const CT<R> *__restrict__ G, CT<R> *__restrict__ Uhat
     if (r == 0) { acc[1] = czero<CT<R>>(); acc[3] = czero<CT<R>>(); }
 #pragma unroll
     for (int p = 0; p < 4; p++) Uhat[unit * 4 * Z3 + p * Z3 + t] = acc[p];
-}
-
-// ---------------------------------------------------------------------------------------------
-// k_bwd_y: inverse y-FFT of one kx column x TC lines, crop y < Ny.  Distributed_FFT.F90:696-788 + :455-476
-template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bwd_y(const CT<R> *__restrict__ Uhat, CT<R> *__restrict__ U1,
-                                                    const CT<R> *__restrict__ tw, int Nx, int Ny, int Nz, int TC)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
-    const int L = 2 * Ny, lg = ilog2(L), ls = L + 1, Z3 = 3 * Nz;
-    const int kx = blockIdx.x, zc0 = blockIdx.y * TC;
-    const int nl = min(TC, Z3 - zc0);
-    if (kx == Nx) return;  // x-Nyquist column is not read by k_bwd_x
-    int q, sx;
-    kx_to_slot(kx, Nx, q, sx);
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-        const int ky = i / nl, t = i - ky * nl;
-        int r, sy;
-        ky_to_slot(ky, Ny, r, sy);
-        s[t * ls + bitrev(ky, lg)] = Uhat[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t];
-    }
-    __syncthreads();
-    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, true);
-    for (int i = threadIdx.x; i < nl * Ny; i += blockDim.x) {
-        const int t = i / Ny, y = i - t * Ny;
-        U1[((size_t)kx * Z3 + zc0 + t) * Ny + y] = s[t * ls + y];
-    }
-}
-
-// ---------------------------------------------------------------------------------------------
-// k_bwd_x: inverse x-FFT, crop x < Nx, post-combine.  apply_ie_operator_module.F90:125-174
-template <typename R>
-__global__ void __launch_bounds__(kThreads) k_bwd_x(const CT<R> *__restrict__ U1, const CT<R> *__restrict__ vin,
-                                                    const CT<R> *__restrict__ asig, const R *__restrict__ post,
-                                                    CT<R> *__restrict__ vout, const CT<R> *__restrict__ tw, int Nx,
-                                                    int Ny, int Nz, int TY)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    CT<R> *s = reinterpret_cast<CT<R> *>(smem_raw);
-    const int L = 2 * Nx, lg = ilog2(L), ls = L + 1, Z3 = 3 * Nz;
-    const int y0 = blockIdx.x * TY, zc = blockIdx.y, z = zc % Nz;
-    const int nl = min(TY, Ny - y0);
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) {
-        const int kx = i / nl, t = i - kx * nl;
-        CT<R> v = czero<CT<R>>();
-        if (kx != Nx) v = U1[((size_t)kx * Z3 + zc) * Ny + y0 + t];
-        s[t * ls + bitrev(kx, lg)] = v;
-    }
-    __syncthreads();
-    smem_fft<CT<R>, false>(s, lg, nl, ls, 1, tw, true);
-    const size_t plane = (size_t)Nx * Ny;
-    const R sq = post[z], inv = post[Nz + z];
-    for (int i = threadIdx.x; i < nl * Nx; i += blockDim.x) {
-        const int t = i / Nx, x = i - t * Nx;
-        const size_t cell = (size_t)z * plane + (size_t)(y0 + t) * Nx + x;
-        const size_t idx = (size_t)zc * plane + (size_t)(y0 + t) * Nx + x;
-        CT<R> d1 = cmul(vin[idx], asig[cell]);
-        CT<R> w = s[t * ls + x];
-        CT<R> o;
-        o.x = (d1.x - w.x * inv) * sq;
-        o.y = (d1.y - w.y * inv) * sq;
-        vout[idx] = o;
-    }
 }
 
 // per-cell coefficients (apply_ie_operator_module.F90:66-68, :134):
@@ -280,18 +284,102 @@ template <> struct Bufs<float> {
     static const float2 *twy(IeOp *o) { return o->d_twy32; }
 };
 
-int pick_lines(int L, size_t elem, int maxlines)
-{
-    // lines per CTA such that the tile stays <= 64 KB of shared memory
-    int n = (int)((64 * 1024) / ((size_t)(L + 1) * elem));
-    if (n < 1) n = 1;
-    if (n > maxlines) n = maxlines;
-    return n;
-}
-
 }  // namespace
 
 int ie_kernel_launch_count_apply() { return 5; }
+
+// lines per CTA: tile of at most ~100 KB of shared memory, power of two, <= 32
+static int lines_for(int L, size_t es)
+{
+    int n = 32;
+    while (n > 1 && (size_t)(n * (L + 1) + L) * es > 100 * 1024) n >>= 1;
+    return n;
+}
+// threads: one per work item of the larger four-step pass, whole warps, at most 256
+static int threads_for(int L, int NL)
+{
+    int n1 = 2, n2 = 2;
+    switch (L) {
+    case 4: n1 = 2; n2 = 2; break;
+    case 8: n1 = 4; n2 = 2; break;
+    case 16: n1 = 4; n2 = 4; break;
+    case 32: n1 = 8; n2 = 4; break;
+    case 64: n1 = 8; n2 = 8; break;
+    case 128: n1 = 16; n2 = 8; break;
+    case 256: n1 = 16; n2 = 16; break;
+    case 512: n1 = 32; n2 = 16; break;
+    default: n1 = 32; n2 = 32; break;
+    }
+    int t = NL * (n1 > n2 ? n1 : n2);
+    t = ((t + 31) / 32) * 32;
+    return t > kThreads ? kThreads : t;
+}
+template <typename K> static void big_smem(K k)
+{
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+template <typename R, int L>
+static void launch_x(bool fwd, IeOp *op, const CT<R> *d_in, CT<R> *d_out, CT<R> *U1, cudaStream_t st)
+{
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
+    const size_t es = sizeof(CT<R>);
+    const int NL = lines_for(L, es), nt = threads_for(L, NL);
+    const size_t sm = (size_t)(NL * (L + 1) + L) * es;
+    dim3 grid((Z3 + NL - 1) / NL, Ny);
+    static bool attr = false;
+    if (!attr) { big_smem(k_fx<R, L>); big_smem(k_bx<R, L>); attr = true; }
+    if (fwd)
+        k_fx<R, L><<<grid, nt, sm, st>>>(d_in, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL);
+    else
+        k_bx<R, L><<<grid, nt, sm, st>>>(U1, d_in, Bufs<R>::asig(op), Bufs<R>::post(op), d_out,
+                                         Bufs<R>::twx(op), Nx, Ny, Nz, NL);
+}
+
+template <typename R, int L>
+static void launch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st)
+{
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
+    const size_t es = sizeof(CT<R>);
+    const int NL = lines_for(L, es), nt = threads_for(L, NL);
+    const size_t sm = (size_t)(NL * (L + 1) + L) * es;
+    dim3 grid((Z3 + NL - 1) / NL, 2 * Nx);
+    static bool attr = false;
+    if (!attr) { big_smem(k_fy<R, L>); big_smem(k_by<R, L>); attr = true; }
+    if (fwd) k_fy<R, L><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL);
+    else k_by<R, L><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL);
+}
+
+template <typename R>
+static void dispatch_x(bool fwd, IeOp *op, const CT<R> *i, CT<R> *o, CT<R> *U1, cudaStream_t st)
+{
+    switch (2 * op->Nx) {
+    case 4: launch_x<R, 4>(fwd, op, i, o, U1, st); break;
+    case 8: launch_x<R, 8>(fwd, op, i, o, U1, st); break;
+    case 16: launch_x<R, 16>(fwd, op, i, o, U1, st); break;
+    case 32: launch_x<R, 32>(fwd, op, i, o, U1, st); break;
+    case 64: launch_x<R, 64>(fwd, op, i, o, U1, st); break;
+    case 128: launch_x<R, 128>(fwd, op, i, o, U1, st); break;
+    case 256: launch_x<R, 256>(fwd, op, i, o, U1, st); break;
+    case 512: launch_x<R, 512>(fwd, op, i, o, U1, st); break;
+    case 1024: launch_x<R, 1024>(fwd, op, i, o, U1, st); break;
+    }
+}
+template <typename R>
+static void dispatch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st)
+{
+    switch (2 * op->Ny) {
+    case 4: launch_y<R, 4>(fwd, op, U1, Uh, st); break;
+    case 8: launch_y<R, 8>(fwd, op, U1, Uh, st); break;
+    case 16: launch_y<R, 16>(fwd, op, U1, Uh, st); break;
+    case 32: launch_y<R, 32>(fwd, op, U1, Uh, st); break;
+    case 64: launch_y<R, 64>(fwd, op, U1, Uh, st); break;
+    case 128: launch_y<R, 128>(fwd, op, U1, Uh, st); break;
+    case 256: launch_y<R, 256>(fwd, op, U1, Uh, st); break;
+    case 512: launch_y<R, 512>(fwd, op, U1, Uh, st); break;
+    case 1024: launch_y<R, 1024>(fwd, op, U1, Uh, st); break;
+    }
+}
 
 template <typename R>
 static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st)
@@ -302,29 +390,17 @@ static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream
     CT<R> *Uh = reinterpret_cast<CT<R> *>(op->scratch.Uhat);
     const CT<R> *G = Bufs<R>::G(op);
     if (!G || !U1 || !Uh) return G2_ERR_STATE;
-    // forward x
-    {
-        const int L = 2 * Nx, TY = pick_lines(L, es, 32);
-        const size_t sm = (size_t)TY * (L + 1) * es;
-        dim3 grid((Ny + TY - 1) / TY, Z3);
-        k_fwd_x<R><<<grid, kThreads, sm, st>>>(d_in, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, TY);
-    }
-    // forward y
-    {
-        const int L = 2 * Ny, TC = pick_lines(L, es, 32);
-        const size_t sm = (size_t)TC * (L + 1) * es;
-        dim3 grid(2 * Nx, (Z3 + TC - 1) / TC);
-        k_fwd_y<R><<<grid, kThreads, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, TC);
-    }
+    dispatch_x<R>(true, op, d_in, nullptr, U1, st);
+    dispatch_y<R>(true, op, U1, Uh, st);
     // contraction
     int rc_fast = G2_ERR_UNSUPPORTED;
     if (op->use_fast_contract) {
         if (sizeof(R) == 8)
             rc_fast = ie_contract_fast64(reinterpret_cast<const double2 *>(G), reinterpret_cast<double2 *>(Uh), Nx, Ny,
-                                         Nz, op->d_err, st);
+                                         Nz, op->d_err, st, op->contract_variant[0]);
         else
             rc_fast = ie_contract_fast32(reinterpret_cast<const float2 *>(G), reinterpret_cast<float2 *>(Uh), Nx, Ny,
-                                         Nz, op->d_err, st);
+                                         Nz, op->d_err, st, op->contract_variant[1]);
         if (rc_fast != G2_OK && rc_fast != G2_ERR_UNSUPPORTED) return rc_fast;
     }
     if (rc_fast != G2_OK) {
@@ -333,21 +409,8 @@ static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream
         const int threads = ((Z3 + 31) / 32) * 32;
         k_contract<R><<<(unsigned)op->units(), threads, sm, st>>>(G, Uh, Nx, Ny, Nz);
     }
-    // inverse y
-    {
-        const int L = 2 * Ny, TC = pick_lines(L, es, 32);
-        const size_t sm = (size_t)TC * (L + 1) * es;
-        dim3 grid(2 * Nx, (Z3 + TC - 1) / TC);
-        k_bwd_y<R><<<grid, kThreads, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, TC);
-    }
-    // inverse x + post
-    {
-        const int L = 2 * Nx, TY = pick_lines(L, es, 32);
-        const size_t sm = (size_t)TY * (L + 1) * es;
-        dim3 grid((Ny + TY - 1) / TY, Z3);
-        k_bwd_x<R><<<grid, kThreads, sm, st>>>(U1, d_in, Bufs<R>::asig(op), Bufs<R>::post(op), d_out,
-                                               Bufs<R>::twx(op), Nx, Ny, Nz, TY);
-    }
+    dispatch_y<R>(false, op, U1, Uh, st);
+    dispatch_x<R>(false, op, d_in, d_out, U1, st);
     G2_CUDA_CHECK(cudaGetLastError());
     return G2_OK;
 }
@@ -366,16 +429,8 @@ static int set_smem_attrs(IeOp *op)
     static bool done = false;
     if (done) return G2_OK;
     const int big = 227 * 1024;
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_x<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_x<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_fwd_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     G2_CUDA_CHECK(cudaFuncSetAttribute(k_contract<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     G2_CUDA_CHECK(cudaFuncSetAttribute(k_contract<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_y<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_y<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_x<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    G2_CUDA_CHECK(cudaFuncSetAttribute(k_bwd_x<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     (void)op;
     done = true;
     return G2_OK;
@@ -390,21 +445,21 @@ int ie_alloc_scratch(IeOp *op)
     return set_smem_attrs(op);
 }
 
-// twiddles exp(-2 pi i j / L), j < L/2, rounded from long double
+// twiddles exp(-2 pi i j / L), j < L, rounded from long double
 static int make_tw(int L, double2 **d64, float2 **d32)
 {
-    std::vector<double2> h64(L / 2);
-    std::vector<float2> h32(L / 2);
+    std::vector<double2> h64(L);
+    std::vector<float2> h32(L);
     const long double pi = 3.141592653589793238462643383279502884L;
-    for (int j = 0; j < L / 2; j++) {
+    for (int j = 0; j < L; j++) {
         long double a = -2.0L * pi * (long double)j / (long double)L;
         h64[j] = make_double2((double)cosl(a), (double)sinl(a));
         h32[j] = make_float2((float)cosl(a), (float)sinl(a));
     }
-    G2_CUDA_CHECK(cudaMalloc(d64, sizeof(double2) * (L / 2)));
-    G2_CUDA_CHECK(cudaMalloc(d32, sizeof(float2) * (L / 2)));
-    G2_CUDA_CHECK(cudaMemcpy(*d64, h64.data(), sizeof(double2) * (L / 2), cudaMemcpyHostToDevice));
-    G2_CUDA_CHECK(cudaMemcpy(*d32, h32.data(), sizeof(float2) * (L / 2), cudaMemcpyHostToDevice));
+    G2_CUDA_CHECK(cudaMalloc(d64, sizeof(double2) * L));
+    G2_CUDA_CHECK(cudaMalloc(d32, sizeof(float2) * L));
+    G2_CUDA_CHECK(cudaMemcpy(*d64, h64.data(), sizeof(double2) * L, cudaMemcpyHostToDevice));
+    G2_CUDA_CHECK(cudaMemcpy(*d32, h32.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
     return G2_OK;
 }
 

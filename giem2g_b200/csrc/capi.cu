@@ -230,7 +230,7 @@ int giem2g_set_ie_kernel_spatial(void *ie, const void *symm, const void *asym)
     return set_status(0);
 }
 
-static int get_units(IeOp *op, const double2 *d, void *symm, void *asym)
+static int get_units(IeOp *op, const double2 *d, void *symm, void *asym, int W = 1)
 {
     const int P = op->P(), Nz = op->Nz, T = op->Tunit();
     const size_t U = op->units();
@@ -240,7 +240,10 @@ static int get_units(IeOp *op, const double2 *d, void *symm, void *asym)
     double2 *s = reinterpret_cast<double2 *>(symm), *a = reinterpret_cast<double2 *>(asym);
     for (size_t u = 0; u < U; u++) {
         std::memcpy(s + u * 4 * P, &h[u * T], sizeof(double2) * 4 * P);
-        std::memcpy(a + u * 2 * Nz * Nz, &h[u * T + 4 * P], sizeof(double2) * 2 * Nz * Nz);
+        for (int blk = 0; blk < 2; blk++)
+            for (int c = 0; c < Nz; c++)
+                for (int r = 0; r < Nz; r++)
+                    a[u * 2 * Nz * Nz + blk * Nz * Nz + c * Nz + r] = h[u * T + 4 * P + blk * Nz * Nz + asw(r, c, Nz, W)];
     }
     return set_status(0);
 }
@@ -256,7 +259,7 @@ int giem2g_get_ie_kernel_spectral(void *ie, void *symm, void *asym)
 {
     IeOp *op = resolve(ie);
     if (!op || !op->have_spectral) return fail(G2_ERR_STATE, "giem2g_get_ie_kernel_spectral: no spectral tensor");
-    return get_units(op, op->d_tensor64, symm, asym);
+    return get_units(op, op->d_tensor64, symm, asym, asw_width64(op->Nz));
 }
 
 void giem2g_calc_fft_of_ie_kernel(void *ie)
@@ -327,6 +330,22 @@ void giem2g_apply_ie_operator(void *ie, void *in, void *out)
     cudaEventElapsedTime(&ms, op->ev0, op->ev1);
     op->apply_seconds += ms * 1e-3;
     set_status(0);
+}
+
+int giem2g_set_contract_variant(void *ie, int precision, int variant)
+{
+    IeOp *op = resolve(ie);
+    if (!op || precision < 0 || precision > 1) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: bad arguments");
+    const int n = ie_contract_variants(precision, op->Nz);
+    if (variant < 0 || (variant > 0 && variant >= n)) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: variant %d of %d", variant, n);
+    op->contract_variant[precision] = variant;
+    return set_status(0);
+}
+
+int giem2g_contract_variants(void *ie, int precision)
+{
+    IeOp *op = resolve(ie);
+    return op ? ie_contract_variants(precision, op->Nz) : 0;
 }
 
 int giem2g_check_device_error(void *ie)

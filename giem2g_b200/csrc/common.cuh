@@ -97,6 +97,14 @@ G2_D void smem_fft(C *s, int log2L, int nlines, int ls, int es, const C *__restr
     }
 }
 
+// Device layout of the full (xz, yz) Nz x Nz blocks: column-major with the row index XOR-swizzled by
+// the low bits of the column, so lane-parallel reads of a row and of a column both hit distinct
+// shared-memory banks.  W = 1 is plain column-major.
+G2_HD int asw(int r, int c, int N, int W) { return c * N + (r ^ (c & (W - 1))); }
+// swizzle widths used for the FP64 and FP32 device tensors
+__host__ __device__ constexpr int asw_width64(int Nz) { return (Nz % 8 == 0) ? 8 : 1; }
+__host__ __device__ constexpr int asw_width32(int Nz) { return (Nz % 16 == 0) ? 16 : ((Nz % 8 == 0) ? 8 : 1); }
+
 #define G2_CUDA_CHECK(expr)                                                                    \
     do {                                                                                       \
         cudaError_t e_ = (expr);                                                               \

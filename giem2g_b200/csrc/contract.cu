@@ -12,8 +12,10 @@
 //   * consumer warps: thread (b, s, z) owns row z of unit b for all 3 components and 4 points and sums
 //     over the j-slice s; complex products use 3 real multiplies (T1=a c, T2=b d, T3=(a+b)(c+d);
 //     re=T1-T2, im=T3-T1-T2), 25% fewer FMAs than 4-multiply complex arithmetic, which matters because
-//     the FP64 contraction sits at the B200 FP64 ridge; slice partials are reduced through the drained
-//     stage buffer; Nyquist points are zeroed as in the reference.
+//     the FP64 contraction sits at the B200 FP64 ridge; FMAs are issued term-major so consecutive ones
+//     update independent accumulators; the 4-point inputs are broadcast reads of the staged spectrum;
+//     slice partials are reduced through the drained stage buffer; Nyquist points are zeroed as in
+//     the reference.
 // Every mbarrier wait is bounded (2 s); on timeout the kernel records an error code and returns after
 // the producer has waited (bounded) for its copies in flight.
 #include "common.cuh"
@@ -34,13 +36,13 @@ struct CfgT {
     static constexpr int TBYTES = B * T * ES;
     static constexpr int UBYTES = B * 4 * Z3 * ES;
     static constexpr int STAGE_BYTES = TBYTES + UBYTES;
-    static constexpr int U3_BYTES = B * 4 * 3 * NZ * 3 * (int)sizeof(R);
     static constexpr int RED_BYTES = S * B * 12 * NZ * ES;
-    static constexpr int SMEM = NSTAGE * STAGE_BYTES + U3_BYTES + 2 * NSTAGE * 8;
+    static constexpr int SMEM = NSTAGE * STAGE_BYTES + 2 * NSTAGE * 8;
     static_assert(NZ % S == 0, "slices must divide Nz");
     static_assert(NC % 32 == 0, "consumer threads must be whole warps");
     static_assert(RED_BYTES <= TBYTES, "reduction buffer reuses the drained tensor stage");
     static_assert(STAGE_BYTES % 16 == 0 && TBYTES % 16 == 0, "bulk copies need 16-byte multiples");
+    static_assert(SMEM <= 232448, "exceeds the 227 KB dynamic shared memory of one CTA");
 };
 
 template <typename R> struct V2;
@@ -57,10 +59,10 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
 {
     using Cfg = CfgT<R, NZ, S, B, NSTAGE>;
     using C2 = typename V2<R>::T;
+    constexpr int AW = sizeof(R) == 8 ? asw_width64(NZ) : asw_width32(NZ);
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *stages = smem;
-    R *u3 = reinterpret_cast<R *>(smem + NSTAGE * Cfg::STAGE_BYTES);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * Cfg::STAGE_BYTES + Cfg::U3_BYTES);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * Cfg::STAGE_BYTES);
     uint64_t *empty = full + NSTAGE;
 
     const int tid = threadIdx.x;
@@ -117,15 +119,6 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
         unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
         const C2 *gt = reinterpret_cast<const C2 *>(st);
         const C2 *uh = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);
-        // inputs in 3-multiply form: u3[b][p][c][j] = (re, im, re+im)
-        for (int i = tid; i < B * 4 * 3 * NZ; i += Cfg::NC) {
-            const C2 v = uh[i];
-            u3[3 * i + 0] = v.x;
-            u3[3 * i + 1] = v.y;
-            u3[3 * i + 2] = v.x + v.y;
-        }
-        named_bar_sync(1, Cfg::NC);
-
         R acc[3][4][3];
 #pragma unroll
         for (int c = 0; c < 3; c++)
@@ -137,46 +130,51 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
         const C2 *gb = gt + b * Cfg::T;
         const C2 *gxx = gb, *gxy = gb + Cfg::P, *gyy = gb + 2 * Cfg::P, *gzz = gb + 3 * Cfg::P;
         const C2 *gxz = gb + 4 * Cfg::P, *gyz = gb + 4 * Cfg::P + NZ * NZ;
-        const R *ub = u3 + b * 4 * 3 * NZ * 3;
+        const C2 *ub = uh + b * 4 * Cfg::Z3;  // [p][c][j], broadcast reads
 #pragma unroll 2
         for (int jj = 0; jj < Cfg::JS; jj++) {
             const int j = s * Cfg::JS + jj;
             const int si = sym_idx<NZ>(z, j);
-            const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[z + j * NZ], gyz[z + j * NZ], gxz[j + z * NZ],
-                             gyz[j + z * NZ]};
-            R es[8];
+            const int a_zj = asw(z, j, NZ, AW), a_jz = asw(j, z, NZ, AW);
+            const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[a_zj], gyz[a_zj], gxz[a_jz], gyz[a_jz]};
+            C2 u[4][3];
+            R ue[4][3];
 #pragma unroll
-            for (int k = 0; k < 8; k++) es[k] = e[k].x + e[k].y;
+            for (int p = 0; p < 4; p++)
 #pragma unroll
-            for (int p = 0; p < 4; p++) {
-                const R sx = (p & 2) ? R(-1) : R(1);
-                const R m = (p & 1) ? R(-1) : R(1);
-                const R *ux = ub + ((p * 3 + 0) * NZ + j) * 3;
-                const R *uy = ub + ((p * 3 + 1) * NZ + j) * 3;
-                const R *uz = ub + ((p * 3 + 2) * NZ + j) * 3;
-                const R xc = ux[0], xd = ux[1], xe = ux[2];
-                const R yc = uy[0], yd = uy[1], ye = uy[2];
-                const R zc = uz[0], zd = uz[1], ze = uz[2];
-#define G2_ACC(C, K, SG, IN_C, IN_D, IN_E)                                 \
-    acc[C][p][0] = fma((SG) * e[K].x, IN_C, acc[C][p][0]);                 \
-    acc[C][p][1] = fma((SG) * e[K].y, IN_D, acc[C][p][1]);                 \
-    acc[C][p][2] = fma((SG) * es[K], IN_E, acc[C][p][2]);
-                // out x: xx Ux + (sx m) xy Uy + sx xz Uz
-                G2_ACC(0, 0, R(1), xc, xd, xe)
-                G2_ACC(0, 1, sx * m, yc, yd, ye)
-                G2_ACC(0, 4, sx, zc, zd, ze)
-                // out y: (sx m) xy Ux + yy Uy + m yz Uz
-                G2_ACC(1, 1, sx * m, xc, xd, xe)
-                G2_ACC(1, 2, R(1), yc, yd, ye)
-                G2_ACC(1, 5, m, zc, zd, ze)
-                // out z: -sx xz^T Ux - m yz^T Uy + zz Uz
-                G2_ACC(2, 6, -sx, xc, xd, xe)
-                G2_ACC(2, 7, -m, yc, yd, ye)
-                G2_ACC(2, 3, R(1), zc, zd, ze)
-#undef G2_ACC
-            }
+                for (int c = 0; c < 3; c++) {
+                    u[p][c] = ub[(p * 3 + c) * NZ + j];
+                    ue[p][c] = u[p][c].x + u[p][c].y;
+                }
+            // term-major: each term updates 12 independent accumulators (4 points x 3 partial products)
+#define G2_TERM(C, K, IN, SGN)                                                   \
+    {                                                                            \
+        const R es_ = e[K].x + e[K].y;                                           \
+        _Pragma("unroll") for (int p = 0; p < 4; p++)                            \
+        {                                                                        \
+            const R sx = (p & 2) ? R(-1) : R(1);                                 \
+            const R m = (p & 1) ? R(-1) : R(1);                                  \
+            const R sg = (SGN);                                                  \
+            acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);           \
+            acc[C][p][1] = fma(sg * e[K].y, u[p][IN].y, acc[C][p][1]);           \
+            acc[C][p][2] = fma(sg * es_, ue[p][IN], acc[C][p][2]);               \
+        }                                                                        \
+    }
+            // out x: xx Ux + (sx m) xy Uy + sx xz Uz
+            // out y: (sx m) xy Ux + yy Uy + m yz Uz
+            // out z: -sx xz^T Ux - m yz^T Uy + zz Uz
+            G2_TERM(0, 0, 0, R(1))
+            G2_TERM(1, 1, 0, sx * m)
+            G2_TERM(2, 6, 0, -sx)
+            G2_TERM(0, 1, 1, sx * m)
+            G2_TERM(1, 2, 1, R(1))
+            G2_TERM(2, 7, 1, -m)
+            G2_TERM(0, 4, 2, sx)
+            G2_TERM(1, 5, 2, m)
+            G2_TERM(2, 3, 2, R(1))
+#undef G2_TERM
         }
-        named_bar_sync(1, Cfg::NC);  // all reads of this stage's tensor and of u3 are done
+        named_bar_sync(1, Cfg::NC);  // all reads of this stage's tensor and inputs are done
         // slice partials into the drained tensor area: red[s][b][p][c][z]
         C2 *red = reinterpret_cast<C2 *>(st);
 #pragma unroll
@@ -242,24 +240,37 @@ int sm_count()
 
 }  // namespace
 
+// Tile-shape variants per (precision, Nz); variant 0 is the default.  The autotuner times the variants
+// on the operator's own buffers and stores its pick in the operator.
+int ie_contract_variants(int precision, int Nz)
+{
+    if (precision == 0) return Nz == 32 ? 2 : (Nz == 8 || Nz == 16 ? 1 : 0);
+    return Nz == 32 ? 3 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
+}
+
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
-int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st)
+int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int v)
 {
     const int n = sm_count();
     switch (Nz) {
     case 8: return launch_cfg<double, 8, 2, 8, 4>(G, Uhat, Nx, Ny, err, n, st);
-    case 16: return launch_cfg<double, 16, 4, 2, 4>(G, Uhat, Nx, Ny, err, n, st);
-    case 32: return launch_cfg<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st);
+    case 16: return launch_cfg<double, 16, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st);
+    case 32:
+        if (v == 1) return launch_cfg<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st);
+        return launch_cfg<double, 32, 8, 1, 3>(G, Uhat, Nx, Ny, err, n, st);
     default: return G2_ERR_UNSUPPORTED;
     }
 }
-int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st)
+int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int v)
 {
     const int n = sm_count();
     switch (Nz) {
-    case 8: return launch_cfg<float, 8, 2, 8, 8>(G, Uhat, Nx, Ny, err, n, st);
-    case 16: return launch_cfg<float, 16, 4, 2, 6>(G, Uhat, Nx, Ny, err, n, st);
-    case 32: return launch_cfg<float, 32, 4, 1, 5>(G, Uhat, Nx, Ny, err, n, st);
+    case 8: return launch_cfg<float, 8, 2, 16, 4>(G, Uhat, Nx, Ny, err, n, st);
+    case 16: return launch_cfg<float, 16, 4, 4, 4>(G, Uhat, Nx, Ny, err, n, st);
+    case 32:
+        if (v == 1) return launch_cfg<float, 32, 4, 1, 5>(G, Uhat, Nx, Ny, err, n, st);
+        if (v == 2) return launch_cfg<float, 32, 8, 2, 3>(G, Uhat, Nx, Ny, err, n, st);
+        return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st);
     case 48: return launch_cfg<float, 48, 4, 1, 2>(G, Uhat, Nx, Ny, err, n, st);
     default: return G2_ERR_UNSUPPORTED;
     }

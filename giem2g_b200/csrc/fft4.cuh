@@ -1,0 +1,113 @@
+// Four-step FFT of many short lines inside one CTA: register DFTs + one shared-memory transpose.
+//
+// A line of length L = N1*N2 (power of two) is transformed as
+//   step 1: thread (line, n1) loads x[n1 + N1*n2], n2 < N2, does an N2-point DFT in registers,
+//           multiplies by W_L^(n1*k2) and parks the N2 values in shared memory;
+//   step 2: thread (line, k2) reads the N1 values of column k2, does an N1-point DFT in registers,
+//           and emits X[k2 + N2*k1].
+// PAD_IN: inputs with index >= L/2 are zero (zero-padded transform) and are neither loaded nor
+// multiplied.  CROP_OUT: only outputs with index < L/2 are produced.
+// Register DFTs are radix-2 decimation-in-frequency with compile-time indexing; every twiddle comes
+// from one table tw[j] = exp(-2 pi i j / L), j < L, held in shared memory.
+#pragma once
+#include "common.cuh"
+
+template <int N> struct Log2 { static constexpr int v = 1 + Log2<N / 2>::v; };
+template <> struct Log2<1> { static constexpr int v = 0; };
+
+__host__ __device__ constexpr int brev_c(int v, int bits)
+{
+    int r = 0;
+    for (int i = 0; i < bits; i++) r |= ((v >> i) & 1) << (bits - 1 - i);
+    return r;
+}
+
+template <typename C, bool INV>
+G2_D C twid(const C *tw, int idx)
+{
+    C w = tw[idx];
+    if (INV) w.y = -w.y;
+    return w;
+}
+
+// In-place N-point DFT of a[] (natural order in, bit-reversed order out).  L/N is the table stride.
+// If HALF_ZERO, a[N/2..N-1] are zero on entry (first stage pruned).
+template <typename C, int N, bool INV, bool HALF_ZERO>
+G2_D void reg_dft_dif(C (&a)[N], const C *tw, int Lstride)
+{
+#pragma unroll
+    for (int h = N / 2; h >= 1; h /= 2) {
+#pragma unroll
+        for (int g = 0; g < N; g += 2 * h) {
+#pragma unroll
+            for (int j = 0; j < h; j++) {
+                const C u = a[g + j];
+                if (HALF_ZERO && h == N / 2) {
+                    a[g + j] = u;
+                    a[g + j + h] = (j == 0) ? u : cmul(u, twid<C, INV>(tw, j * (N / (2 * h)) * Lstride));
+                } else {
+                    const C v = a[g + j + h];
+                    a[g + j] = u + v;
+                    const C d = u - v;
+                    a[g + j + h] = (j == 0) ? d : cmul(d, twid<C, INV>(tw, j * (N / (2 * h)) * Lstride));
+                }
+            }
+        }
+    }
+}
+
+// One CTA transforms `nl` lines.  Functors:
+//   load(line, idx) -> C            (step 1 input)
+//   store(line, idx, C)             (step 2 output)
+//   off(line, n1, k2) -> int        (shared-memory slot of the intermediate)
+// LF1/LF2: item ordering (true: line index fastest across threads; false: n1 / k2 fastest).
+template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
+          class StoreF, class OffF>
+G2_D void fft4step(C *sm, int nl, const C *tw, LoadF load, StoreF store, OffF off)
+{
+    constexpr int L = N1 * N2;
+    const int n_items1 = nl * N1;
+    for (int it = threadIdx.x; it < n_items1; it += blockDim.x) {
+        int line, n1;
+        if (LF1) { line = it % nl; n1 = it / nl; }
+        else { n1 = it % N1; line = it / N1; }
+        C a[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) {
+            if (PAD_IN && n2 >= N2 / 2) a[n2] = czero<C>();
+            else a[n2] = load(line, n1 + N1 * n2);
+        }
+        reg_dft_dif<C, N2, INV, PAD_IN>(a, tw, L / N2);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            C v = a[brev_c(k2, Log2<N2>::v)];
+            if (k2 != 0 && n1 != 0) v = cmul(v, twid<C, INV>(tw, n1 * k2));
+            sm[off(line, n1, k2)] = v;
+        }
+    }
+    __syncthreads();
+    const int n_items2 = nl * N2;
+    for (int it = threadIdx.x; it < n_items2; it += blockDim.x) {
+        int line, k2;
+        if (LF2) { line = it % nl; k2 = it / nl; }
+        else { k2 = it % N2; line = it / N2; }
+        C a[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) a[n1] = sm[off(line, n1, k2)];
+        reg_dft_dif<C, N1, INV, false>(a, tw, L / N1);
+#pragma unroll
+        for (int k1 = 0; k1 < (CROP_OUT ? N1 / 2 : N1); k1++) store(line, k2 + N2 * k1, a[brev_c(k1, Log2<N1>::v)]);
+    }
+}
+
+// factorisation L = N1 * N2 used by the transform kernels
+template <int L> struct Fact;
+template <> struct Fact<4> { static constexpr int N1 = 2, N2 = 2; };
+template <> struct Fact<8> { static constexpr int N1 = 4, N2 = 2; };
+template <> struct Fact<16> { static constexpr int N1 = 4, N2 = 4; };
+template <> struct Fact<32> { static constexpr int N1 = 8, N2 = 4; };
+template <> struct Fact<64> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct Fact<128> { static constexpr int N1 = 16, N2 = 8; };
+template <> struct Fact<256> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Fact<512> { static constexpr int N1 = 32, N2 = 16; };
+template <> struct Fact<1024> { static constexpr int N1 = 32, N2 = 32; };

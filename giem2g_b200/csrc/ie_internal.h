@@ -48,6 +48,7 @@ struct IeOp {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
     bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
+    int contract_variant[2] = {0, 0};  // tile-shape variant per precision (autotuner's pick)
     // counters (Integral_Equation_Module.F90:44-56)
     long long mult_num = 0;
     double apply_seconds = 0;
@@ -71,8 +72,9 @@ int ie_kernel_launch_count_apply();
 int ie_green_tensor(IeOp *op, cudaStream_t st);
 
 // contract.cu: specialised contraction; G2_ERR_UNSUPPORTED when Nz has no specialisation
-int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st);
-int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st);
+int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int variant);
+int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int variant);
+int ie_contract_variants(int precision, int Nz);
 
 // tensor_fft.cu
 int ie_tensor_spectrum(IeOp *op, cudaStream_t st);

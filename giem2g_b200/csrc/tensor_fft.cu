@@ -32,6 +32,15 @@ G2_D void elem_parity(int e, int P, int Nz, double &sx, double &sy)
     }
 }
 
+// position of unit element e in the device layout (full blocks swizzled, see asw)
+G2_HD int dev_pos(int e, int P, int Nz, int W)
+{
+    if (e < 4 * P) return e;
+    const int li = e - 4 * P, blk = li / (Nz * Nz), rc = li - blk * Nz * Nz;
+    const int r = rc % Nz, c = rc / Nz;
+    return 4 * P + blk * Nz * Nz + asw(r, c, Nz, W);
+}
+
 // pass A: spatial [lx][ly][T] -> S1 [kx 0..Nx][ly][T]
 __global__ void __launch_bounds__(kThreads) k_tensor_x(const double2 *__restrict__ g, double2 *__restrict__ S1,
                                                        const double2 *__restrict__ tw, int Nx, int Ny, int Nz)
@@ -92,19 +101,27 @@ __global__ void __launch_bounds__(kThreads) k_tensor_y(const double2 *__restrict
         const double sgn = (ky & 1) ? -1.0 : 1.0;
         double2 v = make_double2(s[ky * TE + t].x - sgn * ny.x, s[ky * TE + t].y - sgn * ny.y);
         if (nyq == nullptr) {
-            out[(size_t)ky * T + e0 + t] = v;  // x-Nyquist row
+            out[(size_t)ky * T + e0 + t] = v;  // x-Nyquist row (plain layout, scratch)
         } else {
             const double sx = (kx & 1) ? -1.0 : 1.0;
             const double2 c = nyq[(size_t)ky * T + e0 + t];
-            out[((size_t)kx * Ny + ky) * T + e0 + t] = make_double2(v.x - sx * c.x, v.y - sx * c.y);
+            out[((size_t)kx * Ny + ky) * T + dev_pos(e0 + t, P, Nz, asw_width64(Nz))] =
+                make_double2(v.x - sx * c.x, v.y - sx * c.y);
         }
     }
 }
 
-__global__ void k_to_c64(const double2 *__restrict__ a, float2 *__restrict__ b, size_t n)
+// complex64 copy; the full blocks move from the FP64 swizzle to the FP32 swizzle
+__global__ void k_to_c64(const double2 *__restrict__ a, float2 *__restrict__ b, size_t units, int P, int Nz)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        b[i] = make_float2((float)a[i].x, (float)a[i].y);
+    const int T = 4 * P + 2 * Nz * Nz, W64 = asw_width64(Nz), W32 = asw_width32(Nz);
+    const size_t n = units * T;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t u = i / T;
+        const int e = (int)(i - u * T);
+        const double2 v = a[u * T + dev_pos(e, P, Nz, W64)];
+        b[u * T + dev_pos(e, P, Nz, W32)] = make_float2((float)v.x, (float)v.y);
+    }
 }
 
 }  // namespace
@@ -126,10 +143,15 @@ int ie_tensor_spectrum(IeOp *op, cudaStream_t st)
     k_tensor_x<<<dim3(Ny, eb), kThreads, smx, st>>>(op->d_spatial, S1, op->d_twx64, Nx, Ny, Nz);
     k_tensor_y<<<dim3(1, eb), kThreads, smy, st>>>(S1, nyq, nullptr, op->d_twy64, Nx, Ny, Nz, Nx);
     k_tensor_y<<<dim3(Nx, eb), kThreads, smy, st>>>(S1, op->d_tensor64, nyq, op->d_twy64, Nx, Ny, Nz, 0);
-    k_to_c64<<<1184, 256, 0, st>>>(op->d_tensor64, op->d_tensor32, n_out);
+    k_to_c64<<<1184, 256, 0, st>>>(op->d_tensor64, op->d_tensor32, op->units(), op->P(), Nz);
     G2_CUDA_CHECK(cudaGetLastError());
     G2_CUDA_CHECK(cudaStreamSynchronize(st));
     cudaFree(S1);
     cudaFree(nyq);
+    // the reference transforms the kernel buffer in place (G_symm and G_symmT alias it), so the
+    // spatial tensor does not outlive the transform there either
+    cudaFree(op->d_spatial);
+    op->d_spatial = nullptr;
+    op->have_spatial = false;
     return G2_OK;
 }

@@ -98,6 +98,10 @@ int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int
 /* Synchronise the operator's stream and report a device-side error word (bounded waits that ran
  * out) as a nonzero status. */
 int giem2g_check_device_error(void *ie);
+/* Contraction tile-shape variants available for a precision (0 or 1) at this Nz, and selection of one
+ * (what the autotuner in giem2g_b200.autotune sets after timing them). */
+int giem2g_contract_variants(void *ie, int precision);
+int giem2g_set_contract_variant(void *ie, int precision, int variant);
 /* CUDA stream the operator's kernels run on (cudaStream_t). */
 void *giem2g_get_stream(void *ie);
 /* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */
