@@ -51,8 +51,9 @@ G2_D void load_tw(C *dst, const C *__restrict__ src, int L)
 template <typename R, int L>
 __global__ void __launch_bounds__(kThreads) k_fx(const CT<R> *__restrict__ vin, const CT<R> *__restrict__ gsig,
                                                  CT<R> *__restrict__ U1, const CT<R> *__restrict__ twg, int Nx,
-                                                 int Ny, int Nz, int NL)
+                                                 int Ny, int Nz, int NL, const int *gate)
 {
+    if (gate && *gate == 0) return;
     using C = CT<R>;
     constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -76,8 +77,10 @@ __global__ void __launch_bounds__(kThreads) k_fx(const CT<R> *__restrict__ vin, 
 // Distributed_FFT.F90:437-505 (y transform + +-ky repack) and :639-694 (+-kx repack)
 template <typename R, int L>
 __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uh,
-                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL)
+                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
+                                                 const int *gate)
 {
+    if (gate && *gate == 0) return;
     using C = CT<R>;
     constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -111,8 +114,10 @@ __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, C
 // k_by: inverse y-FFT of one kx column, crop y < Ny.  Distributed_FFT.F90:455-476, 696-788
 template <typename R, int L>
 __global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, CT<R> *__restrict__ U1,
-                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL)
+                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
+                                                 const int *gate)
 {
+    if (gate && *gate == 0) return;
     using C = CT<R>;
     constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -141,8 +146,9 @@ template <typename R, int L>
 __global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, const CT<R> *__restrict__ vin,
                                                  const CT<R> *__restrict__ asig, const R *__restrict__ post,
                                                  CT<R> *__restrict__ vout, const CT<R> *__restrict__ twg, int Nx,
-                                                 int Ny, int Nz, int NL)
+                                                 int Ny, int Nz, int NL, const int *gate)
 {
+    if (gate && *gate == 0) return;
     using C = CT<R>;
     constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -178,8 +184,10 @@ __global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, c
 // Point signs (sigma_x, m) from slot s: sigma_x = -1 if s&2, m = -1 if s&1:
 //   xy: sigma_x*m   xz: sigma_x   zx: -sigma_x (xz^T)   yz: m   zy: -m (yz^T)   diagonal blocks: +1
 template <typename R>
-__global__ void k_contract(const CT<R> *__restrict__ G, CT<R> *__restrict__ Uhat, int Nx, int Ny, int Nz)
+__global__ void k_contract(const CT<R> *__restrict__ G, CT<R> *__restrict__ Uhat, int Nx, int Ny, int Nz,
+                           const int *gate)
 {
+    if (gate && *gate == 0) return;
     const int AW = sizeof(R) == 8 ? asw_width64(Nz) : asw_width32(Nz);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int P = Nz * (Nz + 1) / 2, T = 4 * P + 2 * Nz * Nz, Z3 = 3 * Nz;
@@ -320,7 +328,8 @@ template <typename K> static void big_smem(K k)
 }
 
 template <typename R, int L>
-static void launch_x(bool fwd, IeOp *op, const CT<R> *d_in, CT<R> *d_out, CT<R> *U1, cudaStream_t st)
+static void launch_x(bool fwd, IeOp *op, const CT<R> *d_in, CT<R> *d_out, CT<R> *U1, cudaStream_t st,
+                     const int *gate)
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
     const size_t es = sizeof(CT<R>);
@@ -330,14 +339,14 @@ static void launch_x(bool fwd, IeOp *op, const CT<R> *d_in, CT<R> *d_out, CT<R> 
     static bool attr = false;
     if (!attr) { big_smem(k_fx<R, L>); big_smem(k_bx<R, L>); attr = true; }
     if (fwd)
-        k_fx<R, L><<<grid, nt, sm, st>>>(d_in, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL);
+        k_fx<R, L><<<grid, nt, sm, st>>>(d_in, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
     else
         k_bx<R, L><<<grid, nt, sm, st>>>(U1, d_in, Bufs<R>::asig(op), Bufs<R>::post(op), d_out,
-                                         Bufs<R>::twx(op), Nx, Ny, Nz, NL);
+                                         Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
 }
 
 template <typename R, int L>
-static void launch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st)
+static void launch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
     const size_t es = sizeof(CT<R>);
@@ -346,43 +355,43 @@ static void launch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st)
     dim3 grid((Z3 + NL - 1) / NL, 2 * Nx);
     static bool attr = false;
     if (!attr) { big_smem(k_fy<R, L>); big_smem(k_by<R, L>); attr = true; }
-    if (fwd) k_fy<R, L><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL);
-    else k_by<R, L><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL);
+    if (fwd) k_fy<R, L><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL, gate);
+    else k_by<R, L><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL, gate);
 }
 
 template <typename R>
-static void dispatch_x(bool fwd, IeOp *op, const CT<R> *i, CT<R> *o, CT<R> *U1, cudaStream_t st)
+static void dispatch_x(bool fwd, IeOp *op, const CT<R> *i, CT<R> *o, CT<R> *U1, cudaStream_t st, const int *gate)
 {
     switch (2 * op->Nx) {
-    case 4: launch_x<R, 4>(fwd, op, i, o, U1, st); break;
-    case 8: launch_x<R, 8>(fwd, op, i, o, U1, st); break;
-    case 16: launch_x<R, 16>(fwd, op, i, o, U1, st); break;
-    case 32: launch_x<R, 32>(fwd, op, i, o, U1, st); break;
-    case 64: launch_x<R, 64>(fwd, op, i, o, U1, st); break;
-    case 128: launch_x<R, 128>(fwd, op, i, o, U1, st); break;
-    case 256: launch_x<R, 256>(fwd, op, i, o, U1, st); break;
-    case 512: launch_x<R, 512>(fwd, op, i, o, U1, st); break;
-    case 1024: launch_x<R, 1024>(fwd, op, i, o, U1, st); break;
+    case 4: launch_x<R, 4>(fwd, op, i, o, U1, st, gate); break;
+    case 8: launch_x<R, 8>(fwd, op, i, o, U1, st, gate); break;
+    case 16: launch_x<R, 16>(fwd, op, i, o, U1, st, gate); break;
+    case 32: launch_x<R, 32>(fwd, op, i, o, U1, st, gate); break;
+    case 64: launch_x<R, 64>(fwd, op, i, o, U1, st, gate); break;
+    case 128: launch_x<R, 128>(fwd, op, i, o, U1, st, gate); break;
+    case 256: launch_x<R, 256>(fwd, op, i, o, U1, st, gate); break;
+    case 512: launch_x<R, 512>(fwd, op, i, o, U1, st, gate); break;
+    case 1024: launch_x<R, 1024>(fwd, op, i, o, U1, st, gate); break;
     }
 }
 template <typename R>
-static void dispatch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st)
+static void dispatch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
 {
     switch (2 * op->Ny) {
-    case 4: launch_y<R, 4>(fwd, op, U1, Uh, st); break;
-    case 8: launch_y<R, 8>(fwd, op, U1, Uh, st); break;
-    case 16: launch_y<R, 16>(fwd, op, U1, Uh, st); break;
-    case 32: launch_y<R, 32>(fwd, op, U1, Uh, st); break;
-    case 64: launch_y<R, 64>(fwd, op, U1, Uh, st); break;
-    case 128: launch_y<R, 128>(fwd, op, U1, Uh, st); break;
-    case 256: launch_y<R, 256>(fwd, op, U1, Uh, st); break;
-    case 512: launch_y<R, 512>(fwd, op, U1, Uh, st); break;
-    case 1024: launch_y<R, 1024>(fwd, op, U1, Uh, st); break;
+    case 4: launch_y<R, 4>(fwd, op, U1, Uh, st, gate); break;
+    case 8: launch_y<R, 8>(fwd, op, U1, Uh, st, gate); break;
+    case 16: launch_y<R, 16>(fwd, op, U1, Uh, st, gate); break;
+    case 32: launch_y<R, 32>(fwd, op, U1, Uh, st, gate); break;
+    case 64: launch_y<R, 64>(fwd, op, U1, Uh, st, gate); break;
+    case 128: launch_y<R, 128>(fwd, op, U1, Uh, st, gate); break;
+    case 256: launch_y<R, 256>(fwd, op, U1, Uh, st, gate); break;
+    case 512: launch_y<R, 512>(fwd, op, U1, Uh, st, gate); break;
+    case 1024: launch_y<R, 1024>(fwd, op, U1, Uh, st, gate); break;
     }
 }
 
 template <typename R>
-static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st)
+static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st, const int *gate)
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
     const size_t es = sizeof(CT<R>);
@@ -390,38 +399,38 @@ static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream
     CT<R> *Uh = reinterpret_cast<CT<R> *>(op->scratch.Uhat);
     const CT<R> *G = Bufs<R>::G(op);
     if (!G || !U1 || !Uh) return G2_ERR_STATE;
-    dispatch_x<R>(true, op, d_in, nullptr, U1, st);
-    dispatch_y<R>(true, op, U1, Uh, st);
+    dispatch_x<R>(true, op, d_in, nullptr, U1, st, gate);
+    dispatch_y<R>(true, op, U1, Uh, st, gate);
     // contraction
     int rc_fast = G2_ERR_UNSUPPORTED;
     if (op->use_fast_contract) {
         if (sizeof(R) == 8)
             rc_fast = ie_contract_fast64(reinterpret_cast<const double2 *>(G), reinterpret_cast<double2 *>(Uh), Nx, Ny,
-                                         Nz, op->d_err, st, op->contract_variant[0]);
+                                         Nz, op->d_err, st, op->contract_variant[0], gate);
         else
             rc_fast = ie_contract_fast32(reinterpret_cast<const float2 *>(G), reinterpret_cast<float2 *>(Uh), Nx, Ny,
-                                         Nz, op->d_err, st, op->contract_variant[1]);
+                                         Nz, op->d_err, st, op->contract_variant[1], gate);
         if (rc_fast != G2_OK && rc_fast != G2_ERR_UNSUPPORTED) return rc_fast;
     }
     if (rc_fast != G2_OK) {
         const int T = op->Tunit();
         const size_t sm = ((size_t)T + 4 * Z3) * es;
         const int threads = ((Z3 + 31) / 32) * 32;
-        k_contract<R><<<(unsigned)op->units(), threads, sm, st>>>(G, Uh, Nx, Ny, Nz);
+        k_contract<R><<<(unsigned)op->units(), threads, sm, st>>>(G, Uh, Nx, Ny, Nz, gate);
     }
-    dispatch_y<R>(false, op, U1, Uh, st);
-    dispatch_x<R>(false, op, d_in, d_out, U1, st);
+    dispatch_y<R>(false, op, U1, Uh, st, gate);
+    dispatch_x<R>(false, op, d_in, d_out, U1, st, gate);
     G2_CUDA_CHECK(cudaGetLastError());
     return G2_OK;
 }
 
-int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st)
+int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, const int *gate)
 {
-    return ie_apply_device<double>(op, d_in, d_out, st);
+    return ie_apply_device<double>(op, d_in, d_out, st, gate);
 }
-int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st)
+int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, const int *gate)
 {
-    return ie_apply_device<float>(op, d_in, d_out, st);
+    return ie_apply_device<float>(op, d_in, d_out, st, gate);
 }
 
 static int set_smem_attrs(IeOp *op)

@@ -357,6 +357,50 @@ int giem2g_check_device_error(void *ie)
     return rc ? rc : set_status(0);
 }
 
+int giem2g_solve_device(void *ie, const void *d_Ebkg, void *d_Esol, const void *d_E0, GIEM2G_FGMRES_CTL ctl,
+                        GIEM2G_RESULT *info)
+{
+    IeOp *op = resolve(ie);
+    int rc = check_ready(op, "giem2g_solve_device");
+    if (rc) return rc;
+    if (!d_Ebkg || !d_Esol || !info) return fail(G2_ERR_ARG, "giem2g_solve_device: NULL argument");
+    rc = krylov_solve_device(op, reinterpret_cast<const double2 *>(d_Ebkg), reinterpret_cast<double2 *>(d_Esol),
+                             reinterpret_cast<const double2 *>(d_E0), ctl, info);
+    if (rc) return fail(rc, "giem2g_solve_device: %s", giem2g_last_error());
+    return set_status(0);
+}
+
+int giem2g_solve(void *ie, const void *E_bkg, void *Esol, const void *E0, GIEM2G_FGMRES_CTL ctl, GIEM2G_RESULT *info)
+{
+    // SolveEquation (ie_solver_module.F90:43-114) with host arrays
+    IeOp *op = resolve(ie);
+    int rc = check_ready(op, "giem2g_solve");
+    if (rc) return rc;
+    if (!E_bkg || !Esol || !info) return fail(G2_ERR_ARG, "giem2g_solve: NULL argument");
+    const size_t nb = op->nvec() * sizeof(double2);
+    double2 *d_e0 = nullptr;
+    if (cudaMemcpyAsync(op->d_vin, E_bkg, nb, cudaMemcpyHostToDevice, op->stream) != cudaSuccess)
+        return fail(G2_ERR_CUDA, "giem2g_solve: copy failed");
+    if (E0) {
+        if (cudaMalloc(&d_e0, nb) != cudaSuccess) return fail(G2_ERR_NOMEM, "giem2g_solve: cudaMalloc failed");
+        cudaMemcpyAsync(d_e0, E0, nb, cudaMemcpyHostToDevice, op->stream);
+    }
+    rc = krylov_solve_device(op, op->d_vin, op->d_vout, d_e0, ctl, info);
+    if (d_e0) cudaFree(d_e0);
+    if (rc) return fail(rc, "giem2g_solve: %s", giem2g_last_error());
+    if (cudaMemcpyAsync(Esol, op->d_vout, nb, cudaMemcpyDeviceToHost, op->stream) != cudaSuccess ||
+        cudaStreamSynchronize(op->stream) != cudaSuccess)
+        return fail(G2_ERR_CUDA, "giem2g_solve: copy back failed");
+    return set_status(0);
+}
+
+int giem2g_get_misfit_history(void *ie, double *out, int max_len)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !out) return 0;
+    return krylov_history(op, out, max_len);
+}
+
 void *giem2g_get_stream(void *ie)
 {
     IeOp *op = resolve(ie);

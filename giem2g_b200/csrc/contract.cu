@@ -55,8 +55,9 @@ G2_D int sym_idx(int i, int j) { return i <= j ? i + j * (j + 1) / 2 : j + i * (
 template <typename R, int NZ, int S, int B, int NSTAGE>
 __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
     k_contract_tma(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
-                   long long nbatches, int *err)
+                   long long nbatches, int *err, const int *gate)
 {
+    if (gate && *gate == 0) return;  // uniform across the CTA: nothing has been issued yet
     using Cfg = CfgT<R, NZ, S, B, NSTAGE>;
     using C2 = typename V2<R>::T;
     constexpr int AW = sizeof(R) == 8 ? asw_width64(NZ) : asw_width32(NZ);
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
 }
 
 template <typename R, int NZ, int S, int B, int NSTAGE>
-int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st)
+int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
     using Cfg = CfgT<R, NZ, S, B, NSTAGE>;
     auto kern = k_contract_tma<R, NZ, S, B, NSTAGE>;
@@ -222,7 +223,7 @@ int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cud
     const long long nb = units / B;
     const int grid = (int)(nb < nsm ? nb : nsm);
     kern<<<grid, Cfg::NTHREADS, Cfg::SMEM, st>>>(reinterpret_cast<const typename V2<R>::T *>(G),
-                                                 reinterpret_cast<typename V2<R>::T *>(Uhat), Ny, nb, err);
+                                                 reinterpret_cast<typename V2<R>::T *>(Uhat), Ny, nb, err, gate);
     G2_CUDA_CHECK(cudaGetLastError());
     return G2_OK;
 }
@@ -249,29 +250,31 @@ int ie_contract_variants(int precision, int Nz)
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
-int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int v)
+int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int v,
+                       const int *gate)
 {
     const int n = sm_count();
     switch (Nz) {
-    case 8: return launch_cfg<double, 8, 2, 8, 4>(G, Uhat, Nx, Ny, err, n, st);
-    case 16: return launch_cfg<double, 16, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st);
+    case 8: return launch_cfg<double, 8, 2, 8, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 16: return launch_cfg<double, 16, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 32:
-        if (v == 1) return launch_cfg<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st);
-        return launch_cfg<double, 32, 8, 1, 3>(G, Uhat, Nx, Ny, err, n, st);
+        if (v == 1) return launch_cfg<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        return launch_cfg<double, 32, 8, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
     }
 }
-int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int v)
+int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int v,
+                       const int *gate)
 {
     const int n = sm_count();
     switch (Nz) {
-    case 8: return launch_cfg<float, 8, 2, 16, 4>(G, Uhat, Nx, Ny, err, n, st);
-    case 16: return launch_cfg<float, 16, 4, 4, 4>(G, Uhat, Nx, Ny, err, n, st);
+    case 8: return launch_cfg<float, 8, 2, 16, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 16: return launch_cfg<float, 16, 4, 4, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 32:
-        if (v == 1) return launch_cfg<float, 32, 4, 1, 5>(G, Uhat, Nx, Ny, err, n, st);
-        if (v == 2) return launch_cfg<float, 32, 8, 2, 3>(G, Uhat, Nx, Ny, err, n, st);
-        return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st);
-    case 48: return launch_cfg<float, 48, 4, 1, 2>(G, Uhat, Nx, Ny, err, n, st);
+        if (v == 1) return launch_cfg<float, 32, 4, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 2) return launch_cfg<float, 32, 8, 2, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 48: return launch_cfg<float, 48, 4, 1, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
     }
 }

@@ -41,6 +41,7 @@ struct IeOp {
     float2 *d_twx32 = nullptr, *d_twy32 = nullptr;
     ApplyScratch scratch;
     int *d_err = nullptr;              // device error word written by bounded waits (0 = ok)
+    void *krylov = nullptr;            // solver workspace (krylov.cu)
     // host staging for the reference-facing (host-pointer) apply
     double2 *h_stage_in = nullptr, *h_stage_out = nullptr;
     double2 *d_vin = nullptr, *d_vout = nullptr;
@@ -62,8 +63,10 @@ struct IeOp {
 };
 
 // apply.cu
-int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st);
-int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st);
+// gate: optional device flag; when it reads 0 every kernel of the apply returns at once (used by the
+// solver to skip Arnoldi steps after convergence without a host round trip)
+int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, const int *gate = nullptr);
+int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, const int *gate = nullptr);
 int ie_alloc_scratch(IeOp *op);
 int ie_make_twiddles(IeOp *op);
 int ie_kernel_launch_count_apply();
@@ -72,8 +75,10 @@ int ie_kernel_launch_count_apply();
 int ie_green_tensor(IeOp *op, cudaStream_t st);
 
 // contract.cu: specialised contraction; G2_ERR_UNSUPPORTED when Nz has no specialisation
-int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int variant);
-int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int variant);
+int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int variant,
+                       const int *gate);
+int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st, int variant,
+                       const int *gate);
 int ie_contract_variants(int precision, int Nz);
 
 // tensor_fft.cu
