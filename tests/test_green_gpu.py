@@ -1,0 +1,80 @@
+"""GPU Green's-tensor construction (giem2g_calc_ie_kernel) against the oracle's restatement of
+CalcIntegralGreenTensor.  The GPU sums the same terms in a different order (lambda-basis GEMM), so
+the tolerance is 1e-10 relative in the 2-norm.
+
+One class of entries is excluded from that bound: xx/xy/yy couplings between cells in DIFFERENT
+background layers.  For lambda below ~1e-10 /m the DXX/DYY/DXY Hankel weights that the FFT
+deconvolution returns are round-off (~1e-14 of their maximum) but their row survives the reference's
+threshold, and COMPUTE_WEIGHTS' lambda scaling divides them by lambda (down to 1e-17 /m).  Within a
+layer the basis cancels those terms; across an interface it does not, so the reference's own values
+there carry amplified round-off of its FFT and libm, reproducible on no other platform.  Those
+entries are bounded instead against the size of the coupling block (5%)."""
+import numpy as np
+import pytest
+
+from giem2g_b200.synthetic import IEModel, THREE_LAYER_SIGMA, THREE_LAYER_THICK, config_small_block, csiga_from_sigma
+from tests.helpers import random_sigma, random_vec, rel, tiny_model
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _models():
+    yield tiny_model(4, 4, 3)
+    yield tiny_model(8, 4, 5, freq=100.0)
+    m, _ = config_small_block()
+    yield m
+    # anomaly crossing the 500 m interface, top below the surface, anisotropic cells
+    z = 100.0 + np.arange(9) * 60.0
+    yield IEModel(8, 4, 8, 70.0, 130.0, z, THREE_LAYER_SIGMA.copy(), THREE_LAYER_THICK.copy(), 0.3)
+    # single-layer background (half-space)
+    yield IEModel(4, 4, 4, 50.0, 50.0, np.arange(5) * 40.0, np.array([0.05]), np.array([]), 3.0)
+
+
+def _cross_layer_mask(L, Nz):
+    """packed-upper mask of (i <= j) pairs whose cells lie in different background layers"""
+    P = Nz * (Nz + 1) // 2
+    mask = np.zeros(P, bool)
+    for j in range(Nz):
+        for i in range(j + 1):
+            mask[i + j * (j + 1) // 2] = L[i + 1] != L[j + 1]
+    return mask
+
+
+@pytest.mark.parametrize("idx", range(5))
+def test_green_tensor_matches_oracle(g2lib, orc, idx):
+    m = list(_models())[idx]
+    S_o, A_o = orc.green_tensor(m)
+    op = g2lib.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    S_g, A_g = op.get_ie_kernel_spatial()
+    cross = _cross_layer_mask(orc.layer_numbers(m), m.Nz)
+    # zz and the full xz/yz blocks: everywhere
+    assert rel(S_g[:, :, 3], S_o[:, :, 3]) < TOL
+    for c in range(2):
+        assert rel(A_g[:, :, c], A_o[:, :, c]) < TOL
+    for c in range(3):  # xx, xy, yy
+        same = ~cross
+        assert rel(S_g[:, :, c][..., same], S_o[:, :, c][..., same]) < TOL
+        if cross.any():
+            scale = np.abs(S_o[:, :, c]).max()
+            assert np.abs(S_g[:, :, c][..., cross] - S_o[:, :, c][..., cross]).max() < 0.05 * scale
+    op.delete()
+
+
+def test_full_pipeline_apply(g2lib, orc):
+    """calc_ie_kernel -> calc_fft_of_ie_kernel -> set_anomaly_conductivity -> apply, all on the GPU."""
+    m, sig = config_small_block()
+    op = g2lib.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    op.calc_fft_of_ie_kernel()
+    csiga = csiga_from_sigma(sig, m.freq)
+    op.set_anomaly_conductivity(csiga)
+    S, A = orc.green_tensor(m)
+    sh, ah = orc.tensor_spectrum(m.Nx, m.Ny, m.Nz, S, A)
+    csigb, sqsigb = orc.background_cells(m)
+    v = random_vec(m, 11)
+    ref = orc.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v)
+    assert rel(op.apply_precond(v), ref) < TOL
+    op.delete()
