@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the IE solve at 128x128x32 on B200 (one JSON line on rank 0).
+
+Workload: the 128x128x32 anomaly (50 x 50 x 25 m cells) over the 3-layer background, seeded
+Gaussian-random-field conductivity (log10 sigma mean -2, std 0.7, correlation 400 m), 0.1 Hz,
+plane-wave sources of both polarisations.  One step = solving both polarisations to outer relative
+residual 1e-6 with the nested FGMRES (outer 30 / inner 10) in mixed precision (complex64 inner
+GMRES, FFTs and tensor; FP64 outer Arnoldi, Hessenberg, residual and true-residual check).
+`value` = whole-job polarisation solves per second with everything resident in HBM; `e2e` = the
+same through the C ABI (giem2g_solve) with pinned host inputs/outputs copied every step.
+Multi-GPU: independent replicas (one process per GPU, no data-path collective); the only
+communication is the barrier and the max-over-ranks of the timing.
+
+--impl reference: the reference's CPU path.  The Fortran/MPI/FFTW reference cannot be built on
+this image, so the CPU restatement in oracle/ (FP64, OpenMP on all host cores) is timed instead:
+each step is one outer FGMRES iteration of the 128x128x32 solve (a bounded sample); the solve
+rate follows from the outer-iteration count of the full FP64 solve done once in set-up.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solve time & IE-apply HBM GB/s at 128×128×32: FP64 vs mixed+learned, rel.res 1e-6"
+UNIT = "solves/s"
+TOL = 1e-6
+OUTER, INNER, MAXRESTART = 30, 10, 100
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _algorithmic_bytes(Nx, Ny, Nz, S):
+    """B_apply = S*(T + 2*N_vec + NxNy*Nz): tensor read, x read + y write, one coefficient per cell."""
+    T = Nx * Ny * (2 * Nz * (Nz + 1) + 2 * Nz * Nz)
+    nvec = 3 * Nx * Ny * Nz
+    return S * (T + 2 * nvec + Nx * Ny * Nz)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for i, n in enumerate(names):
+                    if r[5 + i].lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _profiles_traffic():
+    """DRAM traffic per FP64 apply from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", "ie_apply_128x128x32.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_apply_fp64:"):
+                return int(float(line.split(":")[1]))
+    except Exception:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------------------------------------
+def build_problem():
+    from giem2g_b200.synthetic import config_c2
+    from giem2g_b200.sources import plane_wave_integral
+    m, sig = config_c2(seed=2024)
+    e_y = plane_wave_integral(m, 1)
+    e_x = plane_wave_integral(m, 0)
+    return m, sig, e_y, e_x
+
+
+def cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, nthreads):
+    """Time one outer FGMRES iteration of the oracle's FP64 solver (a bounded sample of the solve)."""
+    import oracle
+    from giem2g_b200.synthetic import csiga_from_sigma
+    from giem2g_b200.sources import plane_wave_integral
+    csiga = csiga_from_sigma(sig, m.freq)
+    csigb, sqsigb = oracle.background_cells(m)
+    E0 = plane_wave_integral(m, 1)
+    t = time.perf_counter()
+    _, info, _ = oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, E0, None, 1, INNER, 1, TOL,
+                              nthreads=nthreads)
+    dt = time.perf_counter() - t
+    return dt, info.applies
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        print(json.dumps({"impl": "reference", "rank": rank, "skipped": "rank 0 runs the CPU reference"}),
+              file=sys.stderr)
+        return 0
+    import oracle
+    from giem2g_b200.synthetic import csiga_from_sigma
+    oracle.build()
+    ncores = os.cpu_count() or 1
+    m, sig, e_y, _ = build_problem()
+    t0 = time.perf_counter()
+    S, A = oracle.green_tensor(m, nthreads=ncores)
+    sh, ah = oracle.tensor_spectrum(m.Nx, m.Ny, m.Nz, S, A, nthreads=ncores)
+    del S, A
+    t_setup = time.perf_counter() - t0
+    csiga = csiga_from_sigma(sig, m.freq)
+    csigb, sqsigb = oracle.background_cells(m)
+    t0 = time.perf_counter()
+    _, info, hist = oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, e_y, None, OUTER, INNER,
+                                 MAXRESTART, TOL, nthreads=ncores)
+    t_full = time.perf_counter() - t0
+    n_outer = max(1, info.iterations)
+    for _ in range(args.warmup):
+        cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, ncores)
+    times = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dt, _ = cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, ncores)
+        times.append(dt)
+    total = time.perf_counter() - t0
+    per_iter = total / args.steps
+    value = 1.0 / (per_iter * n_outer)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded GRF conductivity)",
+        "config": {"workload": "IE solve 128x128x32, 3-layer background, 0.1 Hz, pol EY, FGMRES 30/10, "
+                               "outer rel.res 1e-6, FP64",
+                   "step": "one outer FGMRES iteration of the FP64 solve (bounded sample)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
+                         "sample": f"{args.steps} outer FGMRES iterations (1 + {INNER}+2 + 1 applies each) of the "
+                                   f"oracle FP64 solver; solve = {n_outer} outer iterations (full solve in set-up: "
+                                   f"{t_full:.1f} s, {info.applies} applies)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_setup_s": t_setup, "reference_full_solve_s": t_full, "reference_outer_iterations": n_outer,
+        "note": "Fortran/MPI/FFTW reference is not buildable on this image; the CPU restatement (oracle/) is timed",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import giem2g_b200 as g2
+    from giem2g_b200.synthetic import csiga_from_sigma
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        import datetime
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    m, sig, e_y, e_x = build_problem()
+    op = g2.IEOperator.from_model(m)
+    t0 = time.perf_counter()
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    op.calc_fft_of_ie_kernel()
+    torch.cuda.synchronize()
+    t_tensor = time.perf_counter() - t0
+    op.set_anomaly_sigma(sig, m.freq)
+    stream = torch.cuda.ExternalStream(op.stream)
+    n = op.nvec
+    d_ey = torch.from_numpy(np.ascontiguousarray(e_y).ravel()).to(dev)
+    d_ex = torch.from_numpy(np.ascontiguousarray(e_x).ravel()).to(dev)
+    d_sol_y = torch.empty_like(d_ey)
+    d_sol_x = torch.empty_like(d_ex)
+
+    # contraction tile shape: time the variants once (autotuner) and keep the fastest
+    from giem2g_b200.autotune import autotune_contraction
+    tuned = autotune_contraction(op)
+
+    def solve_pair(prec, tol=TOL):
+        iy = op.solve_device(d_ey.data_ptr(), d_sol_y.data_ptr(), None, tol=tol, max_restart=MAXRESTART,
+                             outer_buf=OUTER, inner_buf=INNER, precision=prec)
+        ix = op.solve_device(d_ex.data_ptr(), d_sol_x.data_ptr(), None, tol=tol, max_restart=MAXRESTART,
+                             outer_buf=OUTER, inner_buf=INNER, precision=prec)
+        return iy, ix
+
+    # FP64 reference solves (plain path) for the comparison and the field error
+    iy64, ix64 = solve_pair(0, tol=1e-8)
+    ref_y, ref_x = d_sol_y.clone(), d_sol_x.clone()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    iy64b, ix64b = solve_pair(0, tol=TOL)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    fp64_pair_ms = ev0.elapsed_time(ev1)
+
+    for _ in range(args.warmup):
+        solve_pair(1)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = g2.kernel_launch_count()
+    infos = []
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            infos.append(solve_pair(1))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = g2.kernel_launch_count() - launches0
+    barrier()
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    t_max = max_over_ranks(t_dev)
+    value = 2.0 * args.steps * world / t_max
+    iy, ix = infos[-1]
+    err_y = (torch.linalg.vector_norm(d_sol_y - ref_y) / torch.linalg.vector_norm(ref_y)).item()
+    err_x = (torch.linalg.vector_norm(d_sol_x - ref_x) / torch.linalg.vector_norm(ref_x)).item()
+
+    # end to end through the public C ABI with pinned host buffers (H2D + solve + D2H each step)
+    h_ey = torch.from_numpy(np.ascontiguousarray(e_y)).pin_memory()
+    h_ex = torch.from_numpy(np.ascontiguousarray(e_x)).pin_memory()
+    h_out = torch.empty_like(h_ey).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        for h_in in (h_ey, h_ex):
+            r = g2.ResultT()
+            rc = g2.lib().giem2g_solve(op.handle, h_in.data_ptr(), h_out.data_ptr(), None,
+                                       op._ctl(TOL, MAXRESTART, OUTER, INNER, 1), g2.ctypes.byref(r))
+            if rc != 0:
+                raise RuntimeError(g2.lib().giem2g_last_error().decode())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_value = 2.0 * args.steps * world / t_e2e
+    vec_bytes = n * 16
+
+    # apply roofline: FP64 and complex64 applies timed with CUDA events on the operator's stream
+    def time_apply(prec, reps=20):
+        dt = torch.complex128 if prec == 0 else torch.complex64
+        x = torch.randn(n, dtype=dt, device=dev)
+        y = torch.empty_like(x)
+        for _ in range(3):
+            op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(reps):
+            op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        return a0.elapsed_time(a1) / reps
+
+    ms64 = time_apply(0)
+    ms32 = time_apply(1)
+    B64 = _algorithmic_bytes(m.Nx, m.Ny, m.Nz, 16)
+    B32 = _algorithmic_bytes(m.Nx, m.Ny, m.Nz, 8)
+    peaks = _peaks()
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    if not peak:
+        peak = 6650.0
+    ach64 = B64 / (ms64 * 1e-3) / 1e9
+    ach32 = B32 / (ms32 * 1e-3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle
+            oracle.build()
+            sh, ah = op.get_ie_kernel_spectral()
+            ncores = os.cpu_count() or 1
+            dt, applies = cpu_outer_iteration_rate(m, sig, sh, ah, iy64b.iterations, ncores)
+            cpu = {"value": 1.0 / (dt * max(1, iy64b.iterations)), "unit": UNIT, "cores": ncores, "kind": "port",
+                   "sample": f"one outer FGMRES iteration ({applies} FP64 applies incl. the initial and final "
+                             f"residual) of the oracle solver at 128x128x32 on {ncores} threads = {dt:.2f} s; "
+                             f"solve = {iy64b.iterations} outer iterations (FP64, tol 1e-6)"}
+        except Exception as exc:  # the CPU baseline is reported, never the target
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 outer",
+            "data": "synthetic (seeded GRF conductivity, plane-wave sources)",
+            "config": {"workload": "IE solve 128x128x32 (50x50x25 m cells), 3-layer background, 0.1 Hz, "
+                                   "pols EY+EX, nested FGMRES 30/10, outer rel.res 1e-6, mixed precision",
+                       "parallelism": f"replicas x{world}", "l2": "working set > L2 (tensor 545 MB c64 + 1.09 GB c128)",
+                       "tensor_build_s": t_tensor, "contract_variants": tuned},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * vec_bytes,
+                    "d2h_bytes_per_step": 2 * vec_bytes},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": ach64, "peak": peak, "unit": "GB/s", "frac": ach64 / peak,
+                         "traffic": _profiles_traffic(), "kernel": "FP64 IE apply (5 kernels; contraction dominant)",
+                         "bytes_per_launch": B64, "ms_per_launch": ms64, "peak_source": peak_src},
+            "apply_c64": {"ms": ms32, "achieved_gbs": ach32, "frac": ach32 / peak, "bytes": B32},
+            "solve": {"mixed_pair_ms": t_max / args.steps * 1e3, "fp64_pair_ms": fp64_pair_ms,
+                      "speedup_vs_fp64_gpu": fp64_pair_ms / (t_max / args.steps * 1e3),
+                      "outer_iterations_mixed": [iy.iterations, ix.iterations],
+                      "outer_iterations_fp64": [iy64b.iterations, ix64b.iterations],
+                      "applies_mixed": [iy.applies_fp64 + iy.applies_fp32, ix.applies_fp64 + ix.applies_fp32],
+                      "true_rel_residual_mixed": [iy.be, ix.be],
+                      "field_error_vs_fp64_tol1e-8": [err_y, err_x]},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    op.delete()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_b200(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -68,7 +68,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_get_ie_kernel_spatial", "giem2g_get_ie_kernel_spectral", "giem2g_apply_ie_operator_device",
     "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_solve",
     "giem2g_solve_device", "giem2g_get_misfit_history", "giem2g_check_device_error",
-    "giem2g_contract_variants", "giem2g_set_contract_variant",
+    "giem2g_contract_variants", "giem2g_set_contract_variant", "giem2g_kernel_launch_count",
 ]
 
 
@@ -118,9 +118,15 @@ def lib():
     L.giem2g_get_misfit_history.argtypes = [vp, vp, ip]
     L.giem2g_check_device_error.argtypes = [vp]
     L.giem2g_contract_variants.argtypes = [vp, ip]
+    L.giem2g_kernel_launch_count.restype = ctypes.c_longlong
     L.giem2g_set_contract_variant.argtypes = [vp, ip, ip]
     _lib = L
     return L
+
+
+def kernel_launch_count() -> int:
+    """Cumulative count of this library's kernel launches in this process."""
+    return int(lib().giem2g_kernel_launch_count())
 
 
 def _check(rc=None, what=""):

@@ -1,0 +1,63 @@
+"""Autotuner for the contraction tile shape.
+
+The contraction kernel has several compile-time tile shapes (j-slices per unit, units per stage,
+pipeline depth) per precision and Nz (giem2g_contract_variants).  The best one depends on Nz, the
+precision and the grid, so the tuner times every variant with CUDA events on the operator's own
+buffers (a few full applies each) and keeps the fastest in the operator; results are cached per
+(Nx, Ny, Nz, precision) in a JSON file next to this module when one is given.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+
+def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> dict:
+    import torch
+
+    key = f"{op.Nx}x{op.Ny}x{op.Nz}"
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        try:
+            cache = json.load(open(cache_path))
+        except Exception:
+            cache = {}
+    stream = torch.cuda.ExternalStream(op.stream)
+    picks = {}
+    for prec, dt in ((0, torch.complex128), (1, torch.complex64)):
+        nv = op.contract_variants(prec)
+        if nv <= 1:
+            picks[prec] = {"variant": 0, "ms": None}
+            continue
+        ck = f"{key}:{prec}"
+        if ck in cache:
+            op.set_contract_variant(prec, cache[ck]["variant"])
+            picks[prec] = cache[ck]
+            continue
+        x = torch.randn(op.nvec, dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        best = None
+        for v in range(nv):
+            op.set_contract_variant(prec, v)
+            for _ in range(2):
+                op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            if best is None or ms < best[1]:
+                best = (v, ms)
+        op.set_contract_variant(prec, best[0])
+        picks[prec] = {"variant": best[0], "ms": best[1]}
+        cache[ck] = picks[prec]
+    op.check_device_error()
+    if cache_path:
+        try:
+            json.dump(cache, open(cache_path, "w"), indent=1)
+        except Exception:
+            pass
+    return {str(k): v for k, v in picks.items()}

@@ -420,6 +420,7 @@ static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream
     }
     dispatch_y<R>(false, op, U1, Uh, st, gate);
     dispatch_x<R>(false, op, d_in, d_out, U1, st, gate);
+    g2_count_launches(5);
     G2_CUDA_CHECK(cudaGetLastError());
     return G2_OK;
 }

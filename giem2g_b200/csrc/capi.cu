@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include "common.cuh"
@@ -44,6 +45,9 @@ int get_layer(double z, int Nl, const std::vector<double> &depth)
 }
 }  // namespace
 
+static std::atomic<long long> g_launches{0};
+void g2_count_launches(int n) { g_launches += n; }
+
 void g2_log(const char *msg)
 {
     if (g_logger) g_logger(msg);
@@ -75,6 +79,7 @@ static int fail(int rc, const char *fmt, ...)
 extern "C" {
 
 int giem2g_last_status(void) { return g_last_status; }
+long long giem2g_kernel_launch_count(void) { return g_launches.load(); }
 const char *giem2g_last_error(void) { return g_last_error.c_str(); }
 
 void giem2g_calc_data_sizes(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE *data)

@@ -523,14 +523,14 @@ template <typename C>
 static void dots(KrylovWork *k, const C *V, int K, const C *w, double2 *out, double *nrm2, const int *g1,
                  const int *g2, cudaStream_t st)
 {
-    k_dots<C><<<k->nparts, kVT, 0, st>>>(V, k->N, K, w, k->N, k->part, g1 ? g1 : g2);
-    k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, K, out, nrm2, g1, g2);
+    k_dots<C><<<k->nparts, kVT, 0, st>>>(V, k->N, K, w, k->N, k->part, g1 ? g1 : g2); g2_count_launches(1);
+    k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, K, out, nrm2, g1, g2); g2_count_launches(1);
 }
 template <typename C>
 static void norm2(KrylovWork *k, const C *w, double *nrm2, const int *g, cudaStream_t st)
 {
-    k_dots<C><<<k->nparts, kVT, 0, st>>>(w, k->N, 0, w, k->N, k->part, g);
-    k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, 0, nullptr, nrm2, g, nullptr);
+    k_dots<C><<<k->nparts, kVT, 0, st>>>(w, k->N, 0, w, k->N, k->part, g); g2_count_launches(1);
+    k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, 0, nullptr, nrm2, g, nullptr); g2_count_launches(1);
 }
 
 // CGS for Arnoldi step j on level L with basis V (j+1 columns) and vector w
@@ -539,11 +539,11 @@ static void cgs(KrylovWork *k, Level &L, const C *V, int j, C *w, const int *gat
 {
     const int K = j + 1;
     dots<C>(k, V, K, w, L.hnext, nullptr, gate, nullptr, st);
-    k_cgs_first<<<1, 1, 0, st>>>(L, j, gate);
+    k_cgs_first<<<1, 1, 0, st>>>(L, j, gate); g2_count_launches(1);
     for (int p = 1; p <= N_IGS + 1; p++) {
-        k_cgs_pass<C><<<k->nparts, kVT, 0, st>>>(V, k->N, K, w, k->N, L.hpass, k->part, gate, L.flags + F_PASS);
-        k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, K, L.hnext, L.scal + S_NRM2, gate, L.flags + F_PASS);
-        k_cgs_next<<<1, 1, 0, st>>>(L, j, p, gate);
+        k_cgs_pass<C><<<k->nparts, kVT, 0, st>>>(V, k->N, K, w, k->N, L.hpass, k->part, gate, L.flags + F_PASS); g2_count_launches(1);
+        k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, K, L.hnext, L.scal + S_NRM2, gate, L.flags + F_PASS); g2_count_launches(1);
+        k_cgs_next<<<1, 1, 0, st>>>(L, j, p, gate); g2_count_launches(1);
     }
 }
 
@@ -566,9 +566,9 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
     const int g = vec_grid(N);
     CI *Vi = reinterpret_cast<CI *>(k->Vi), *ri = reinterpret_cast<CI *>(k->ri), *wi = reinterpret_cast<CI *>(k->wi);
     const int *solver = L.flags + F_SOLVER, *krylov = L.flags + F_KRYLOV;
-    k_zero_level<<<1, 256, 0, st>>>(L);
+    k_zero_level<<<1, 256, 0, st>>>(L); g2_count_launches(1);
     norm2<CI>(k, v, L.scal + S_NRM2, nullptr, st);
-    k_set_bn<<<1, 1, 0, st>>>(L);
+    k_set_bn<<<1, 1, 0, st>>>(L); g2_count_launches(1);
     k_copy_or_zero<CI><<<g, kVT, 0, st>>>(x, v, L.scal, N);  // x = x0, or 0 when ||b|| < 1e-14
     int rc = apply_prec<CI>(op, v, ri, st, solver);
     if (rc) return rc;
@@ -576,9 +576,9 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
     k->applies64 += sizeof(CI) == 16 ? 1 : 0;
     k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(ri, 1.0, v, -1.0, ri, N, solver);  // r0 = b - A x0
     norm2<CI>(k, ri, L.scal + S_NRM2, solver, st);
-    k_set_beta<<<1, 1, 0, st>>>(L, tol);
-    k_cycle_start<<<1, 1, 0, st>>>(L, solver);
-    k_scale_by<CI><<<g, kVT, 0, st>>>(Vi, ri, L.scal, S_BETA, N, solver);
+    k_set_beta<<<1, 1, 0, st>>>(L, tol); g2_count_launches(1);
+    k_cycle_start<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
+    k_scale_by<CI><<<g, kVT, 0, st>>>(Vi, ri, L.scal, S_BETA, N, solver); g2_count_launches(1);
     for (int j = 0; j < k->mi; j++) {
         CI *Vj = Vi + (size_t)j * N;
         rc = apply_prec<CI>(op, Vj, wi, st, krylov);
@@ -586,12 +586,12 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
         k->applies32 += sizeof(CI) == 8 ? 1 : 0;
         k->applies64 += sizeof(CI) == 16 ? 1 : 0;
         cgs<CI>(k, L, Vi, j, wi, krylov, st);
-        k_scale_by<CI><<<g, kVT, 0, st>>>(Vi + (size_t)(j + 1) * N, wi, L.scal, S_DNORMW, N, krylov);
-        k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, krylov);
+        k_scale_by<CI><<<g, kVT, 0, st>>>(Vi + (size_t)(j + 1) * N, wi, L.scal, S_DNORMW, N, krylov); g2_count_launches(1);
+        k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, krylov); g2_count_launches(1);
     }
     // FinalActions -> ConstructCurrentSolution (gmres.F90:423-458): x = x0 + V y
-    k_trisolve<<<1, 1, 0, st>>>(L, solver);
-    k_lincomb<CI, CI><<<g, kVT, 0, st>>>(x, 1.0, x, Vi, N, L.y, L.flags + F_L, N, solver);
+    k_trisolve<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
+    k_lincomb<CI, CI><<<g, kVT, 0, st>>>(x, 1.0, x, Vi, N, L.y, L.flags + F_L, N, solver); g2_count_launches(1);
     if (true_residual) {  // gmres.F90:402-419, result unused by the outer solver
         rc = apply_prec<CI>(op, x, ri, st, solver);
         if (rc) return rc;
@@ -625,9 +625,9 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
     info->bea = -1.0;
     info->be = -1.0;
     // gmres.F90:129-168
-    k_zero_level<<<1, 256, 0, st>>>(L);
+    k_zero_level<<<1, 256, 0, st>>>(L); g2_count_launches(1);
     norm2<double2>(k, k->b, L.scal + S_NRM2, nullptr, st);
-    k_set_bn<<<1, 1, 0, st>>>(L);
+    k_set_bn<<<1, 1, 0, st>>>(L); g2_count_launches(1);
     int rc = pull();
     if (rc) return rc;
     if (h_scal[S_BN] < ZERO_THRESHOLD) {
@@ -639,10 +639,10 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
     rc = ie_apply_device64(op, k->x, k->r0, st);  // x holds x0
     if (rc) return rc;
     k->applies64++;
-    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, N, nullptr);
-    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->w, 1.0, k->r0, 0.0, (const double2 *)nullptr, N, nullptr);
+    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, N, nullptr); g2_count_launches(1);
+    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->w, 1.0, k->r0, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
     norm2<double2>(k, k->w, L.scal + S_NRM2, nullptr, st);
-    k_set_beta<<<1, 1, 0, st>>>(L, tol);
+    k_set_beta<<<1, 1, 0, st>>>(L, tol); g2_count_launches(1);
     if ((rc = pull())) return rc;
     if (h_scal[S_BETA] / bn < tol) {
         info->stat = 1;
@@ -654,8 +654,8 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
     double bea = -1.0;
     char msg[256];
     for (;;) {
-        k_cycle_start<<<1, 1, 0, st>>>(L, nullptr);
-        k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo, k->w, L.scal, S_BETA, N, nullptr);
+        k_cycle_start<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+        k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo, k->w, L.scal, S_BETA, N, nullptr); g2_count_launches(1);
         for (int j = 0; j < M; j++) {
             const double2 *Vj = k->Vo + (size_t)j * N;
             CI *Zj = Z + (size_t)j * N;
@@ -664,15 +664,15 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
                 if ((rc = inner_solve<CI>(op, k, reinterpret_cast<const CI *>(Vj), Zj, tol, true_res, st))) return rc;
                 if ((rc = ie_apply_device64(op, reinterpret_cast<const double2 *>(Zj), k->w, st))) return rc;
             } else {
-                k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(vin, 1.0, Vj, 0.0, (const double2 *)nullptr, N, nullptr);
+                k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(vin, 1.0, Vj, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
                 if ((rc = inner_solve<CI>(op, k, vin, Zj, tol, true_res, st))) return rc;
-                k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, N, nullptr);
+                k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, N, nullptr); g2_count_launches(1);
                 if ((rc = ie_apply_device64(op, k->tmp, k->w, st))) return rc;
             }
             k->applies64++;
             cgs<double2>(k, L, k->Vo, j, k->w, nullptr, st);
-            k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo + (size_t)(j + 1) * N, k->w, L.scal, S_DNORMW, N, nullptr);
-            k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, nullptr);
+            k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo + (size_t)(j + 1) * N, k->w, L.scal, S_DNORMW, N, nullptr); g2_count_launches(1);
+            k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, nullptr); g2_count_launches(1);
             if ((rc = pull())) return rc;
             bea = h_scal[S_BEA];
             if (!std::isfinite(bea)) {
@@ -691,20 +691,20 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
         iter++;
         if (iter >= ctl.fgmres_maxit) break;
         // PrepareRestart: x += Z y; w = V g' (gmres.F90:333-379)
-        k_trisolve<<<1, 1, 0, st>>>(L, nullptr);
-        k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, N, L.y, L.flags + F_L, N, nullptr);
-        k_restart_g<<<1, 1, 0, st>>>(L);
-        k_copy_g<<<1, 64, 0, st>>>(L);
+        k_trisolve<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+        k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, N, L.y, L.flags + F_L, N, nullptr); g2_count_launches(1);
+        k_restart_g<<<1, 1, 0, st>>>(L); g2_count_launches(1);
+        k_copy_g<<<1, 64, 0, st>>>(L); g2_count_launches(1);
         k_lincomb<double2, double2><<<g, kVT, 0, st>>>(k->w, 0.0, (const double2 *)nullptr, k->Vo, N, L.y,
                                                        L.flags + F_L, N, nullptr);
     }
     (void)L_used;
     // FinalActions (gmres.F90:382-421)
-    k_trisolve<<<1, 1, 0, st>>>(L, nullptr);
-    k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, N, L.y, L.flags + F_L, N, nullptr);
+    k_trisolve<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+    k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, N, L.y, L.flags + F_L, N, nullptr); g2_count_launches(1);
     if ((rc = ie_apply_device64(op, k->x, k->r0, st))) return rc;
     k->applies64++;
-    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, N, nullptr);
+    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, N, nullptr); g2_count_launches(1);
     norm2<double2>(k, k->r0, L.scal + S_NRM2, nullptr, st);
     if ((rc = pull())) return rc;
     const double be = std::sqrt(h_scal[S_NRM2]) / bn;
@@ -736,14 +736,18 @@ int krylov_solve_device(IeOp *op, const double2 *d_Ebkg, double2 *d_Esol, const 
     cudaEventCreate(&e1);
     cudaEventRecord(e0, st);
     // SolveEquation (ie_solver_module.F90:62-80): rhs = sqrt(Re sb) E_bkg; guess = E0/a or rhs
-    k_rhs<<<g, 256, 0, st>>>(k->b, d_Ebkg, op->d_post64, (size_t)op->Nx * op->Ny, op->Nz);
-    if (d_E0) k_scale_asig<<<g, 256, 0, st>>>(k->x, d_E0, op->d_asig64, cells, true);
-    else cudaMemcpyAsync(k->x, k->b, sizeof(double2) * k->N, cudaMemcpyDeviceToDevice, st);
+    k_rhs<<<g, 256, 0, st>>>(k->b, d_Ebkg, op->d_post64, (size_t)op->Nx * op->Ny, op->Nz); g2_count_launches(1);
+    if (d_E0) {
+        k_scale_asig<<<g, 256, 0, st>>>(k->x, d_E0, op->d_asig64, cells, true);
+        g2_count_launches(1);
+    } else {
+        cudaMemcpyAsync(k->x, k->b, sizeof(double2) * k->N, cudaMemcpyDeviceToDevice, st);
+    }
     if (ctl.precision == 0) rc = outer_solve<double2>(op, k, ctl, info, st);
     else rc = outer_solve<float2>(op, k, ctl, info, st);
     if (rc) return rc;
     // Esol = a * chi (ie_solver_module.F90:85-97)
-    k_scale_asig<<<g, 256, 0, st>>>(d_Esol, k->x, op->d_asig64, cells, false);
+    k_scale_asig<<<g, 256, 0, st>>>(d_Esol, k->x, op->d_asig64, cells, false); g2_count_launches(1);
     cudaEventRecord(e1, st);
     G2_CUDA_CHECK(cudaStreamSynchronize(st));
     float ms = 0;

@@ -80,6 +80,8 @@ void giem2g_delete_ie_operator(void *ie);
 /* ---- status ---------------------------------------------------------------- */
 int giem2g_last_status(void);
 const char *giem2g_last_error(void);
+/* Cumulative number of kernels this library has launched (all operators, this process). */
+long long giem2g_kernel_launch_count(void);
 
 /* ---- extensions -------------------------------------------------------------- */
 /* Background only (PreparePreconditioner, calc_ie_tensor_module.F90:295-306):
