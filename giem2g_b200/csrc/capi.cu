@@ -47,6 +47,7 @@ int get_layer(double z, int Nl, const std::vector<double> &depth)
 
 static std::atomic<long long> g_launches{0};
 void g2_count_launches(int n) { g_launches += n; }
+long long g2_launch_total() { return g_launches.load(); }
 
 void g2_log(const char *msg)
 {

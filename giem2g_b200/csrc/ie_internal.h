@@ -89,6 +89,7 @@ int ie_prepare_sigma(IeOp *op, cudaStream_t st);
 
 int ie_check_device_error(IeOp *op);  // reads d_err after a sync; nonzero -> G2_ERR_NUMERIC
 void g2_count_launches(int n);          // cumulative count of this library's kernel launches
+long long g2_launch_total();
 void g2_log(const char *msg);
 void g2_set_error(const char *file, int line, const char *msg);
 void g2_set_error_msg(const std::string &msg);

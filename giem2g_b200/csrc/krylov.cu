@@ -44,39 +44,6 @@ struct Level {
 
 G2_HD int hix(int i, int j, int m) { return i + j * (m + 1); }
 
-// ------------------------------------------------------------------------------------------------
-// block reduction of K complex values (+ one real) per thread into part[blockIdx.x][0..K], part[..][KMAX]
-template <int KM>
-G2_D void block_reduce_store(double2 (&acc)[KM], double nrm, int K, double2 *part)
-{
-    __shared__ double2 red[kVT / 32][KM + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < KM; k++) {
-        if (k < K) {
-            double2 v = acc[k];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-                v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-            }
-            if (lane == 0) red[warp][k] = v;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
-    if (lane == 0) red[warp][KM] = make_double2(nrm, 0.0);
-    __syncthreads();
-    if (threadIdx.x <= KM && (threadIdx.x < K || threadIdx.x == KM)) {
-        double2 s = make_double2(0.0, 0.0);
-        for (int w = 0; w < kVT / 32; w++) {
-            s.x += red[w][threadIdx.x].x;
-            s.y += red[w][threadIdx.x].y;
-        }
-        part[(size_t)blockIdx.x * (KMAX + 1) + (threadIdx.x == KM ? KMAX : threadIdx.x)] = s;
-    }
-}
-
 template <typename C> G2_D double2 ld2(const C *p, size_t i);
 template <> G2_D double2 ld2<double2>(const double2 *p, size_t i) { return p[i]; }
 template <> G2_D double2 ld2<float2>(const float2 *p, size_t i)
@@ -88,94 +55,123 @@ template <typename C> G2_D void st2(C *p, size_t i, double2 v);
 template <> G2_D void st2<double2>(double2 *p, size_t i, double2 v) { p[i] = v; }
 template <> G2_D void st2<float2>(float2 *p, size_t i, double2 v) { p[i] = make_float2((float)v.x, (float)v.y); }
 
+template <typename C> struct RealOf;
+template <> struct RealOf<double2> { using T = double; };
+template <> struct RealOf<float2> { using T = float; };
+
+// per-thread partial sums in the vector's precision (a handful of elements each), block and grid
+// reductions in FP64
+template <int KM, typename R>
+G2_D void block_reduce_store_r(R (&ax)[KM + 1], R (&ay)[KM + 1], double2 *part)
+{
+    __shared__ double2 red[kVT / 32][KM + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k <= KM; k++) {
+        double vx = ax[k], vy = ay[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            vx += __shfl_xor_sync(0xffffffffu, vx, o);
+            vy += __shfl_xor_sync(0xffffffffu, vy, o);
+        }
+        if (lane == 0) red[warp][k] = make_double2(vx, vy);
+    }
+    __syncthreads();
+    if (threadIdx.x <= KM) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int w = 0; w < kVT / 32; w++) {
+            s.x += red[w][threadIdx.x].x;
+            s.y += red[w][threadIdx.x].y;
+        }
+        part[(size_t)blockIdx.x * (KMAX + 1) + (threadIdx.x == KM ? KMAX : threadIdx.x)] = s;
+    }
+}
+
 // dots: part[b][k] = sum_i conj(V_k[i]) w[i], k < K; part[b][KMAX] = sum |w|^2
-template <typename C>
-__global__ void __launch_bounds__(kVT) k_dots(const C *__restrict__ V, size_t ld, int K, const C *__restrict__ w,
-                                              size_t N, double2 *part, const int *gate)
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_dots_t(const C *__restrict__ V, size_t ld, const C *__restrict__ w,
+                                                size_t N, double2 *part, const int *gate)
 {
     if (gate && *gate == 0) return;
-    double2 acc[KMAX];
+    using R = typename RealOf<C>::T;
+    R ax[K + 1], ay[K + 1];
 #pragma unroll
-    for (int k = 0; k < KMAX; k++) acc[k] = make_double2(0.0, 0.0);
-    double nrm = 0.0;
+    for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
     for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
-        const double2 wv = ld2(w, i);
-        nrm += wv.x * wv.x + wv.y * wv.y;
+        const C wv = w[i];
+        ax[K] += wv.x * wv.x + wv.y * wv.y;
 #pragma unroll
-        for (int k = 0; k < KMAX; k++)
-            if (k < K) {
-                const double2 v = ld2(V, (size_t)k * ld + i);
-                acc[k].x += v.x * wv.x + v.y * wv.y;
-                acc[k].y += v.x * wv.y - v.y * wv.x;
-            }
+        for (int k = 0; k < K; k++) {
+            const C v = V[(size_t)k * ld + i];
+            ax[k] += v.x * wv.x + v.y * wv.y;
+            ay[k] += v.x * wv.y - v.y * wv.x;
+        }
     }
-    block_reduce_store<KMAX>(acc, nrm, K, part);
+    block_reduce_store_r<K, R>(ax, ay, part);
 }
 
 // fused CGS pass: w -= V h; then part[b][k] = sum conj(V_k) w', part[b][KMAX] = ||w'||^2
-template <typename C>
-__global__ void __launch_bounds__(kVT) k_cgs_pass(const C *__restrict__ V, size_t ld, int K, C *__restrict__ w,
-                                                  size_t N, const double2 *__restrict__ h, double2 *part,
-                                                  const int *gate1, const int *gate2)
+// (V is read twice per element; the second read hits L1)
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_cgs_pass_t(const C *__restrict__ V, size_t ld, C *__restrict__ w, size_t N,
+                                                    const double2 *__restrict__ h, double2 *part, const int *gate1,
+                                                    const int *gate2)
 {
     if ((gate1 && *gate1 == 0) || (gate2 && *gate2 == 0)) return;
-    __shared__ double2 hs[KMAX];
+    using R = typename RealOf<C>::T;
+    constexpr int KA = K > 0 ? K : 1;
+    __shared__ double2 hs[KA];
     if (threadIdx.x < K) hs[threadIdx.x] = h[threadIdx.x];
     __syncthreads();
-    double2 acc[KMAX];
+    R ax[K + 1], ay[K + 1];
 #pragma unroll
-    for (int k = 0; k < KMAX; k++) acc[k] = make_double2(0.0, 0.0);
-    double nrm = 0.0;
+    for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
     for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
-        double2 v[KMAX];
-        double2 wv = ld2(w, i);
+        C wv = w[i];
 #pragma unroll
-        for (int k = 0; k < KMAX; k++)
-            if (k < K) {
-                v[k] = ld2(V, (size_t)k * ld + i);
-                wv.x -= v[k].x * hs[k].x - v[k].y * hs[k].y;
-                wv.y -= v[k].x * hs[k].y + v[k].y * hs[k].x;
-            }
-        st2(w, i, wv);
-        const double2 wr = ld2(w, i);  // the stored (possibly rounded) value enters the next dots
-        nrm += wr.x * wr.x + wr.y * wr.y;
+        for (int k = 0; k < K; k++) {
+            const C v = V[(size_t)k * ld + i];
+            const R hx = (R)hs[k].x, hy = (R)hs[k].y;  // shared-memory broadcast
+            wv.x -= v.x * hx - v.y * hy;
+            wv.y -= v.x * hy + v.y * hx;
+        }
+        w[i] = wv;
+        ax[K] += wv.x * wv.x + wv.y * wv.y;
 #pragma unroll
-        for (int k = 0; k < KMAX; k++)
-            if (k < K) {
-                acc[k].x += v[k].x * wr.x + v[k].y * wr.y;
-                acc[k].y += v[k].x * wr.y - v[k].y * wr.x;
-            }
+        for (int k = 0; k < K; k++) {
+            const C v = V[(size_t)k * ld + i];
+            ax[k] += v.x * wv.x + v.y * wv.y;
+            ay[k] += v.x * wv.y - v.y * wv.x;
+        }
     }
-    block_reduce_store<KMAX>(acc, nrm, K, part);
+    block_reduce_store_r<K, R>(ax, ay, part);
 }
 
-// sum the block partials: out[k] = sum_b part[b][k] (k < K), *nrm2 = sum_b part[b][KMAX]
+// sum the block partials, one CTA per column: out[k] = sum_b part[b][k] (k < K), *nrm2 = sum_b part[b][KMAX]
 __global__ void k_reduce_parts(const double2 *__restrict__ part, int nb, int K, double2 *out, double *nrm2,
                                const int *gate1, const int *gate2)
 {
     if ((gate1 && *gate1 == 0) || (gate2 && *gate2 == 0)) return;
     __shared__ double2 sm[256];
-    for (int k = 0; k <= K; k++) {
-        const int col = (k == K) ? KMAX : k;
-        double2 s = make_double2(0.0, 0.0);
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            s.x += part[(size_t)b * (KMAX + 1) + col].x;
-            s.y += part[(size_t)b * (KMAX + 1) + col].y;
-        }
-        sm[threadIdx.x] = s;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o) {
-                sm[threadIdx.x].x += sm[threadIdx.x + o].x;
-                sm[threadIdx.x].y += sm[threadIdx.x + o].y;
-            }
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            if (k < K) out[k] = sm[0];
-            else if (nrm2) *nrm2 = sm[0].x;
+    const int k = blockIdx.x;
+    const int col = (k == K) ? KMAX : k;
+    double2 s = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        s.x += part[(size_t)b * (KMAX + 1) + col].x;
+        s.y += part[(size_t)b * (KMAX + 1) + col].y;
+    }
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sm[threadIdx.x].x += sm[threadIdx.x + o].x;
+            sm[threadIdx.x].y += sm[threadIdx.x + o].y;
         }
         __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (k < K) out[k] = sm[0];
+        else if (nrm2) *nrm2 = sm[0].x;
     }
 }
 
@@ -444,8 +440,14 @@ struct KrylovWork {
     double2 *Vo = nullptr, *x = nullptr, *b = nullptr, *r0 = nullptr, *w = nullptr, *tmp = nullptr;
     void *Zo = nullptr;  // complex128 (plain) or complex64 (mixed)
     // inner
-    void *Vi = nullptr, *ri = nullptr, *wi = nullptr, *vin = nullptr;
+    void *Vi = nullptr, *ri = nullptr, *wi = nullptr, *vin = nullptr, *xin = nullptr;
     Level Lo, Li;
+    // the inner GMRES cycle as a CUDA graph (fixed buffers vin -> xin), captured on its second use
+    cudaGraphExec_t inner_exec = nullptr;
+    double inner_tol = -1.0;
+    int inner_uses = 0, inner_graph_applies = 0, inner_graph_launches = 0;
+    bool inner_true_res = false;
+    int inner_cv[2] = {-1, -1};  // contraction variants baked into the captured graph
     double2 *part = nullptr;
     int nparts = 0;
     std::vector<double> history;
@@ -479,7 +481,8 @@ void krylov_free(IeOp *op)
 {
     KrylovWork *k = reinterpret_cast<KrylovWork *>(op->krylov);
     if (!k) return;
-    void *p[] = {k->Vo, k->x, k->b, k->r0, k->w, k->tmp, k->Zo, k->Vi, k->ri, k->wi, k->vin, k->part};
+    if (k->inner_exec) cudaGraphExecDestroy(k->inner_exec);
+    void *p[] = {k->Vo, k->x, k->b, k->r0, k->w, k->tmp, k->Zo, k->Vi, k->ri, k->wi, k->vin, k->xin, k->part};
     for (void *q : p)
         if (q) cudaFree(q);
     free_level(k->Lo);
@@ -511,6 +514,7 @@ static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
     G2_CUDA_CHECK(cudaMalloc(&k->ri, ei * N));
     G2_CUDA_CHECK(cudaMalloc(&k->wi, ei * N));
     G2_CUDA_CHECK(cudaMalloc(&k->vin, ei * N));
+    G2_CUDA_CHECK(cudaMalloc(&k->xin, ei * N));
     k->nparts = vec_grid(N);
     G2_CUDA_CHECK(cudaMalloc(&k->part, sizeof(double2) * (size_t)k->nparts * (KMAX + 1)));
     int rc = alloc_level(k->Lo, mo);
@@ -519,17 +523,50 @@ static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
 }
 
 // ---- launch helpers ------------------------------------------------------------------------------
+template <typename C, int K>
+static void launch_dots_k(KrylovWork *k, const C *V, const C *w, const int *g, cudaStream_t st)
+{
+    k_dots_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, k->part, g);
+}
+template <typename C, int K>
+static void launch_cgs_k(KrylovWork *k, const C *V, C *w, const double2 *h, const int *g1, const int *g2,
+                         cudaStream_t st)
+{
+    k_cgs_pass_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, h, k->part, g1, g2);
+}
+#define G2_KCASES(F, ...)                                                                                     \
+    switch (K) {                                                                                          \
+    case 0: F<C, 0>(__VA_ARGS__); break; case 1: F<C, 1>(__VA_ARGS__); break;                             \
+    case 2: F<C, 2>(__VA_ARGS__); break; case 3: F<C, 3>(__VA_ARGS__); break;                             \
+    case 4: F<C, 4>(__VA_ARGS__); break; case 5: F<C, 5>(__VA_ARGS__); break;                             \
+    case 6: F<C, 6>(__VA_ARGS__); break; case 7: F<C, 7>(__VA_ARGS__); break;                             \
+    case 8: F<C, 8>(__VA_ARGS__); break; case 9: F<C, 9>(__VA_ARGS__); break;                             \
+    case 10: F<C, 10>(__VA_ARGS__); break; case 11: F<C, 11>(__VA_ARGS__); break;                         \
+    case 12: F<C, 12>(__VA_ARGS__); break; case 13: F<C, 13>(__VA_ARGS__); break;                         \
+    case 14: F<C, 14>(__VA_ARGS__); break; case 15: F<C, 15>(__VA_ARGS__); break;                         \
+    case 16: F<C, 16>(__VA_ARGS__); break; case 17: F<C, 17>(__VA_ARGS__); break;                         \
+    case 18: F<C, 18>(__VA_ARGS__); break; case 19: F<C, 19>(__VA_ARGS__); break;                         \
+    case 20: F<C, 20>(__VA_ARGS__); break; case 21: F<C, 21>(__VA_ARGS__); break;                         \
+    case 22: F<C, 22>(__VA_ARGS__); break; case 23: F<C, 23>(__VA_ARGS__); break;                         \
+    case 24: F<C, 24>(__VA_ARGS__); break; case 25: F<C, 25>(__VA_ARGS__); break;                         \
+    case 26: F<C, 26>(__VA_ARGS__); break; case 27: F<C, 27>(__VA_ARGS__); break;                         \
+    case 28: F<C, 28>(__VA_ARGS__); break; case 29: F<C, 29>(__VA_ARGS__); break;                         \
+    case 30: F<C, 30>(__VA_ARGS__); break; case 31: F<C, 31>(__VA_ARGS__); break;                         \
+    default: F<C, 32>(__VA_ARGS__); break;                                                                \
+    }
+
 template <typename C>
 static void dots(KrylovWork *k, const C *V, int K, const C *w, double2 *out, double *nrm2, const int *g1,
                  const int *g2, cudaStream_t st)
 {
-    k_dots<C><<<k->nparts, kVT, 0, st>>>(V, k->N, K, w, k->N, k->part, g1 ? g1 : g2); g2_count_launches(1);
-    k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, K, out, nrm2, g1, g2); g2_count_launches(1);
+    G2_KCASES(launch_dots_k, k, V, w, g1 ? g1 : g2, st)
+    g2_count_launches(1);
+    k_reduce_parts<<<K + 1, 256, 0, st>>>(k->part, k->nparts, K, out, nrm2, g1, g2); g2_count_launches(1);
 }
 template <typename C>
 static void norm2(KrylovWork *k, const C *w, double *nrm2, const int *g, cudaStream_t st)
 {
-    k_dots<C><<<k->nparts, kVT, 0, st>>>(w, k->N, 0, w, k->N, k->part, g); g2_count_launches(1);
+    k_dots_t<C, 0><<<k->nparts, kVT, 0, st>>>(w, k->N, w, k->N, k->part, g); g2_count_launches(1);
     k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, 0, nullptr, nrm2, g, nullptr); g2_count_launches(1);
 }
 
@@ -541,8 +578,9 @@ static void cgs(KrylovWork *k, Level &L, const C *V, int j, C *w, const int *gat
     dots<C>(k, V, K, w, L.hnext, nullptr, gate, nullptr, st);
     k_cgs_first<<<1, 1, 0, st>>>(L, j, gate); g2_count_launches(1);
     for (int p = 1; p <= N_IGS + 1; p++) {
-        k_cgs_pass<C><<<k->nparts, kVT, 0, st>>>(V, k->N, K, w, k->N, L.hpass, k->part, gate, L.flags + F_PASS); g2_count_launches(1);
-        k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, K, L.hnext, L.scal + S_NRM2, gate, L.flags + F_PASS); g2_count_launches(1);
+        G2_KCASES(launch_cgs_k, k, V, w, L.hpass, gate, L.flags + F_PASS, st)
+        g2_count_launches(1);
+        k_reduce_parts<<<K + 1, 256, 0, st>>>(k->part, k->nparts, K, L.hnext, L.scal + S_NRM2, gate, L.flags + F_PASS); g2_count_launches(1);
         k_cgs_next<<<1, 1, 0, st>>>(L, j, p, gate); g2_count_launches(1);
     }
 }
@@ -598,6 +636,62 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
         k->applies32 += sizeof(CI) == 8 ? 1 : 0;
         k->applies64 += sizeof(CI) == 16 ? 1 : 0;
     }
+    return G2_OK;
+}
+
+// inner solve vin -> xin; eager on first use, then captured once and replayed as a CUDA graph
+template <typename CI>
+static int inner_solve_fixed(IeOp *op, KrylovWork *k, double tol, bool true_res, cudaStream_t st)
+{
+    const CI *v = reinterpret_cast<const CI *>(k->vin);
+    CI *x = reinterpret_cast<CI *>(k->xin);
+    const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
+    const bool graphs = !(ng && ng[0] == '1');
+    if (k->inner_exec && (k->inner_tol != tol || k->inner_true_res != true_res ||
+                          k->inner_cv[0] != op->contract_variant[0] || k->inner_cv[1] != op->contract_variant[1])) {
+        cudaGraphExecDestroy(k->inner_exec);
+        k->inner_exec = nullptr;
+        k->inner_uses = 0;
+    }
+    if (k->inner_exec) {
+        G2_CUDA_CHECK(cudaGraphLaunch(k->inner_exec, st));
+        g2_count_launches(k->inner_graph_launches);
+        if (sizeof(CI) == 8) k->applies32 += k->inner_graph_applies;
+        else k->applies64 += k->inner_graph_applies;
+        return G2_OK;
+    }
+    if (!graphs || k->inner_uses++ == 0) return inner_solve<CI>(op, k, v, x, tol, true_res, st);
+    // capture: count what one cycle launches, then instantiate
+    const int a32 = k->applies32, a64 = k->applies64;
+    const long long l0 = g2_launch_total();
+    cudaGraph_t graph = nullptr;
+    G2_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = inner_solve<CI>(op, k, v, x, tol, true_res, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (rc) return rc;
+    if (ce != cudaSuccess) {
+        g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
+        return G2_ERR_CUDA;
+    }
+    k->inner_graph_applies = (k->applies32 - a32) + (k->applies64 - a64);
+    k->inner_graph_launches = (int)(g2_launch_total() - l0);
+    k->applies32 = a32;
+    k->applies64 = a64;
+    ce = cudaGraphInstantiate(&k->inner_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+        g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
+        k->inner_exec = nullptr;
+        return G2_ERR_CUDA;
+    }
+    k->inner_tol = tol;
+    k->inner_true_res = true_res;
+    k->inner_cv[0] = op->contract_variant[0];
+    k->inner_cv[1] = op->contract_variant[1];
+    G2_CUDA_CHECK(cudaGraphLaunch(k->inner_exec, st));
+    g2_count_launches(k->inner_graph_launches);
+    if (sizeof(CI) == 8) k->applies32 += k->inner_graph_applies;
+    else k->applies64 += k->inner_graph_applies;
     return G2_OK;
 }
 
@@ -659,13 +753,14 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
         for (int j = 0; j < M; j++) {
             const double2 *Vj = k->Vo + (size_t)j * N;
             CI *Zj = Z + (size_t)j * N;
-            // right preconditioner: Z_j = inner GMRES(V_j)  (gmres.F90:251, :491-506)
+            // right preconditioner: Z_j = inner GMRES(V_j)  (gmres.F90:251, :491-506), through the fixed
+            // buffers vin -> xin of the captured inner cycle
+            k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(vin, 1.0, Vj, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
+            if ((rc = inner_solve_fixed<CI>(op, k, tol, true_res, st))) return rc;
+            k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, N, nullptr); g2_count_launches(1);
             if (sizeof(CI) == sizeof(double2)) {
-                if ((rc = inner_solve<CI>(op, k, reinterpret_cast<const CI *>(Vj), Zj, tol, true_res, st))) return rc;
                 if ((rc = ie_apply_device64(op, reinterpret_cast<const double2 *>(Zj), k->w, st))) return rc;
             } else {
-                k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(vin, 1.0, Vj, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
-                if ((rc = inner_solve<CI>(op, k, vin, Zj, tol, true_res, st))) return rc;
                 k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, N, nullptr); g2_count_launches(1);
                 if ((rc = ie_apply_device64(op, k->tmp, k->w, st))) return rc;
             }
