@@ -223,6 +223,7 @@ def run_b200(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    g2.set_logger(lambda msg: print(msg, file=sys.stderr))  # stdout carries the one JSON line
     m, sig, e_y, e_x = build_problem()
     op = g2.IEOperator.from_model(m)
     t0 = time.perf_counter()
@@ -383,7 +384,7 @@ def run_b200(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

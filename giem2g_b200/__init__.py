@@ -124,6 +124,17 @@ def lib():
     return L
 
 
+LOGGER_FN = ctypes.CFUNCTYPE(None, ctypes.c_char_p)
+_logger_ref = None
+
+
+def set_logger(fn=None):
+    """giem2g_set_logger (giem2g_interfaces.F90:234-238): fn(str) receives every log line; None = stdout."""
+    global _logger_ref
+    _logger_ref = LOGGER_FN(lambda b: fn(b.decode(errors="replace"))) if fn else None
+    lib().giem2g_set_logger(_logger_ref)
+
+
 def kernel_launch_count() -> int:
     """Cumulative count of this library's kernel launches in this process."""
     return int(lib().giem2g_kernel_launch_count())
