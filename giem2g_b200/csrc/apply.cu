@@ -390,13 +390,14 @@ static void dispatch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st
     }
 }
 
+// The five kernels over the scratch pair (U1, Uh); every element of both is written before it is
+// read, so neither has to start at zero.
 template <typename R>
-static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st, const int *gate)
+static int ie_apply_core(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st, const int *gate, CT<R> *U1,
+                         CT<R> *Uh)
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
     const size_t es = sizeof(CT<R>);
-    CT<R> *U1 = reinterpret_cast<CT<R> *>(op->scratch.U1);
-    CT<R> *Uh = reinterpret_cast<CT<R> *>(op->scratch.Uhat);
     const CT<R> *G = Bufs<R>::G(op);
     if (!G || !U1 || !Uh) return G2_ERR_STATE;
     dispatch_x<R>(true, op, d_in, nullptr, U1, st, gate);
@@ -425,6 +426,13 @@ static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream
     return G2_OK;
 }
 
+template <typename R>
+static int ie_apply_device(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t st, const int *gate)
+{
+    return ie_apply_core<R>(op, d_in, d_out, st, gate, reinterpret_cast<CT<R> *>(op->scratch.U1),
+                            reinterpret_cast<CT<R> *>(op->scratch.Uhat));
+}
+
 int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, const int *gate)
 {
     return ie_apply_device<double>(op, d_in, d_out, st, gate);
@@ -432,6 +440,23 @@ int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_
 int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, const int *gate)
 {
     return ie_apply_device<float>(op, d_in, d_out, st, gate);
+}
+
+size_t ie_apply_scratch_elems(const IeOp *op, size_t *n_u1)
+{
+    const size_t u1 = (size_t)2 * op->Nx * 3 * op->Nz * op->Ny;
+    if (n_u1) *n_u1 = u1;
+    return u1 + (size_t)op->Nx * op->Ny * 4 * 3 * op->Nz;
+}
+int ie_apply_device64_scratch(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, double2 *U1,
+                              double2 *Uhat)
+{
+    return ie_apply_core<double>(op, d_in, d_out, st, nullptr, U1, Uhat);
+}
+int ie_apply_device32_scratch(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, float2 *U1,
+                              float2 *Uhat)
+{
+    return ie_apply_core<float>(op, d_in, d_out, st, nullptr, U1, Uhat);
 }
 
 static int set_smem_attrs(IeOp *op)

@@ -320,6 +320,42 @@ int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int
     return set_status(0);
 }
 
+// Same result as giem2g_apply_ie_operator_device, with the apply's intermediates in the library's
+// static device array (static_scratch.cu) instead of the operator's buffers: the call allocates
+// nothing.  Rejects grids whose intermediates exceed the array.
+int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_out, int precision)
+{
+    IeOp *op = resolve(ie);
+    int rc = check_ready(op, "giem2g_apply_ie_operator_device_static");
+    if (rc) return rc;
+    if (precision != 0 && precision != 1)
+        return fail(G2_ERR_ARG, "giem2g_apply_ie_operator_device_static: precision must be 0 or 1");
+    void *base = nullptr;
+    size_t cap = 0, n_u1 = 0;
+    rc = ie_static_scratch(&base, &cap);
+    if (rc) return fail(rc, "giem2g_apply_ie_operator_device_static: static scratch set-up failed: %s",
+                        giem2g_last_error());
+    const size_t es = precision == 0 ? sizeof(double2) : sizeof(float2);
+    const size_t n_all = ie_apply_scratch_elems(op, &n_u1);
+    const size_t off_uh = (n_u1 * es + 255) / 256 * 256;
+    const size_t need = off_uh + (n_all - n_u1) * es;
+    if (need > cap)
+        return fail(G2_ERR_ARG,
+                    "giem2g_apply_ie_operator_device_static: grid %dx%dx%d needs %zu bytes of scratch at precision "
+                    "%d, above the static maximum of %zu bytes; use giem2g_apply_ie_operator_device",
+                    op->Nx, op->Ny, op->Nz, need, precision, cap);
+    unsigned char *b = static_cast<unsigned char *>(base);
+    if (precision == 0)
+        rc = ie_apply_device64_scratch(op, reinterpret_cast<const double2 *>(d_in), reinterpret_cast<double2 *>(d_out),
+                                       op->stream, reinterpret_cast<double2 *>(b),
+                                       reinterpret_cast<double2 *>(b + off_uh));
+    else
+        rc = ie_apply_device32_scratch(op, reinterpret_cast<const float2 *>(d_in), reinterpret_cast<float2 *>(d_out),
+                                       op->stream, reinterpret_cast<float2 *>(b), reinterpret_cast<float2 *>(b + off_uh));
+    if (rc) return fail(rc, "giem2g_apply_ie_operator_device_static: %s", giem2g_last_error());
+    return set_status(0);
+}
+
 void giem2g_apply_ie_operator(void *ie, void *in, void *out)
 {
     // apply_ie_operator_module.F90:39 via giem2g_interfaces.F90:203-232: host vectors in/out

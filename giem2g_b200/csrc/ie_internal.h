@@ -67,6 +67,15 @@ struct IeOp {
 // solver to skip Arnoldi steps after convergence without a host round trip)
 int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, const int *gate = nullptr);
 int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, const int *gate = nullptr);
+// The same apply over caller-given scratch (U1: first n_u1 elements, Uhat: the rest).
+size_t ie_apply_scratch_elems(const IeOp *op, size_t *n_u1);
+int ie_apply_device64_scratch(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, double2 *U1,
+                              double2 *Uhat);
+int ie_apply_device32_scratch(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, float2 *U1,
+                              float2 *Uhat);
+// Process-wide static scratch of the static-scratch apply: device address (set-up on first use per
+// device) and capacity in bytes.
+int ie_static_scratch(void **ptr, size_t *capacity);
 int ie_alloc_scratch(IeOp *op);
 int ie_make_twiddles(IeOp *op);
 int ie_kernel_launch_count_apply();

@@ -97,6 +97,14 @@ int giem2g_get_ie_kernel_spectral(void *ie, void *symm_hat, void *asym_hat);
 /* Device-pointer apply on the operator's stream.  precision 0: complex128 vectors and
  * FP64 tensor; precision 1: complex64 vectors and tensor (FP32 accumulation). */
 int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int precision);
+/* No counterpart in the reference.  The same apply as giem2g_apply_ie_operator_device, but it
+ * allocates nothing: the apply's intermediates live in one static device array of the library
+ * (32 MiB per device, shared by every call and operator on that device) instead of the operator's
+ * buffers.  For hosts that must not allocate device memory after start-up.  Grids that need more
+ * than 32 MiB of intermediates (18*Nx*Ny*Nz complex of the precision) are rejected with status
+ * -1 and a message.  The first call on a device sets up the array's address; make it before any stream
+ * capture on that device.  Calls that overlap on the GPU race on the shared array. */
+int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_out, int precision);
 /* Synchronise the operator's stream and report a device-side error word (bounded waits that ran
  * out) as a nonzero status. */
 int giem2g_check_device_error(void *ie);
