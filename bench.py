@@ -5,9 +5,10 @@ Workload: the 128x128x32 anomaly (50 x 50 x 25 m cells) over the 3-layer backgro
 Gaussian-random-field conductivity (log10 sigma mean -2, std 0.7, correlation 400 m), 0.1 Hz,
 plane-wave sources of both polarisations.  One step = solving both polarisations to outer relative
 residual 1e-6 with the nested FGMRES (outer 30 / inner 10) in mixed precision (complex64 inner
-GMRES, FFTs and tensor; FP64 outer Arnoldi, Hessenberg, residual and true-residual check).
+GMRES, FFTs and tensor; FP64 outer Arnoldi, Hessenberg, residual and true-residual check), the two
+polarisations as one batch (lockstep solves whose complex64 applies share each tensor read).
 `value` = whole-job polarisation solves per second with everything resident in HBM; `e2e` = the
-same through the C ABI (giem2g_solve) with pinned host inputs/outputs copied every step.
+same through the C ABI (giem2g_solve_batched) with pinned host inputs/outputs copied every step.
 Multi-GPU: independent replicas (one process per GPU, no data-path collective); the only
 communication is the barrier and the max-over-ranks of the timing.
 
@@ -258,8 +259,23 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.synchronize()
     fp64_pair_ms = ev0.elapsed_time(ev1)
 
+    # mixed precision, one polarisation after the other (the reference's order)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    iy_s, ix_s = solve_pair(1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    mixed_seq_pair_ms = ev0.elapsed_time(ev1)
+
+    # the product path: both polarisations as one batch (lockstep FGMRES, paired complex64 applies)
+    batch = g2.Batch([op, op], outer_buf=OUTER, inner_buf=INNER, precision=1, max_restart=MAXRESTART)
+    d_in, d_out = [d_ey.data_ptr(), d_ex.data_ptr()], [d_sol_y.data_ptr(), d_sol_x.data_ptr()]
+
+    def solve_batch():
+        return batch.solve_device(d_in, d_out, tol=TOL)
+
     for _ in range(args.warmup):
-        solve_pair(1)
+        solve_batch()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -268,7 +284,7 @@ def run_b200(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
-            infos.append(solve_pair(1))
+            infos.append(solve_batch())
         ev1.record(stream)
         torch.cuda.synchronize()
     launches = g2.kernel_launch_count() - launches0
@@ -280,21 +296,22 @@ def run_b200(args, rank, world, local_rank):
     err_y = (torch.linalg.vector_norm(d_sol_y - ref_y) / torch.linalg.vector_norm(ref_y)).item()
     err_x = (torch.linalg.vector_norm(d_sol_x - ref_x) / torch.linalg.vector_norm(ref_x)).item()
 
-    # end to end through the public C ABI with pinned host buffers (H2D + solve + D2H each step)
+    # end to end through the public C ABI (giem2g_solve_batched) with pinned host buffers:
+    # H2D of both right-hand sides + solve + D2H of both solutions each step
     h_ey = torch.from_numpy(np.ascontiguousarray(e_y)).pin_memory()
     h_ex = torch.from_numpy(np.ascontiguousarray(e_x)).pin_memory()
-    h_out = torch.empty_like(h_ey).pin_memory()
+    h_oy = torch.empty_like(h_ey).pin_memory()
+    h_ox = torch.empty_like(h_ex).pin_memory()
+    res = (g2.ResultT * 2)()
+    ins, outs = g2._ptrs([h_ey.data_ptr(), h_ex.data_ptr()]), g2._ptrs([h_oy.data_ptr(), h_ox.data_ptr()])
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        for h_in in (h_ey, h_ex):
-            r = g2.ResultT()
-            rc = g2.lib().giem2g_solve(op.handle, h_in.data_ptr(), h_out.data_ptr(), None,
-                                       op._ctl(TOL, MAXRESTART, OUTER, INNER, 1), g2.ctypes.byref(r))
-            if rc != 0:
-                raise RuntimeError(g2.lib().giem2g_last_error().decode())
+        rc = g2.lib().giem2g_solve_batched(batch.handle, ins, outs, None, batch._ctl(TOL), res)
+        if rc != 0:
+            raise RuntimeError(g2.lib().giem2g_last_error().decode())
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
@@ -351,7 +368,7 @@ def run_b200(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 outer",
             "data": "synthetic (seeded GRF conductivity, plane-wave sources)",
             "config": {"workload": "IE solve 128x128x32 (50x50x25 m cells), 3-layer background, 0.1 Hz, "
-                                   "pols EY+EX, nested FGMRES 30/10, outer rel.res 1e-6, mixed precision",
+                                   "pols EY+EX batched, nested FGMRES 30/10, outer rel.res 1e-6, mixed precision",
                        "parallelism": f"replicas x{world}", "l2": "working set > L2 (tensor 545 MB c64 + 1.09 GB c128)",
                        "tensor_build_s": t_tensor, "contract_variants": tuned},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * vec_bytes,
@@ -361,9 +378,11 @@ def run_b200(args, rank, world, local_rank):
                          "traffic": _profiles_traffic(), "kernel": "FP64 IE apply (5 kernels; contraction dominant)",
                          "bytes_per_launch": B64, "ms_per_launch": ms64, "peak_source": peak_src},
             "apply_c64": {"ms": ms32, "achieved_gbs": ach32, "frac": ach32 / peak, "bytes": B32},
-            "solve": {"mixed_pair_ms": t_max / args.steps * 1e3, "fp64_pair_ms": fp64_pair_ms,
+            "solve": {"mixed_batched_pair_ms": t_max / args.steps * 1e3, "mixed_sequential_pair_ms": mixed_seq_pair_ms,
+                      "fp64_pair_ms": fp64_pair_ms,
                       "speedup_vs_fp64_gpu": fp64_pair_ms / (t_max / args.steps * 1e3),
                       "outer_iterations_mixed": [iy.iterations, ix.iterations],
+                      "outer_iterations_mixed_sequential": [iy_s.iterations, ix_s.iterations],
                       "outer_iterations_fp64": [iy64b.iterations, ix64b.iterations],
                       "applies_mixed": [iy.applies_fp64 + iy.applies_fp32, ix.applies_fp64 + ix.applies_fp32],
                       "true_rel_residual_mixed": [iy.be, ix.be],
@@ -372,6 +391,7 @@ def run_b200(args, rank, world, local_rank):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
+    batch.delete()
     op.delete()
     if dist:
         dist.destroy_process_group()

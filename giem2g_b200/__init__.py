@@ -69,6 +69,9 @@ EXPORTED_SYMBOLS = [
     "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_solve",
     "giem2g_solve_device", "giem2g_get_misfit_history", "giem2g_check_device_error",
     "giem2g_contract_variants", "giem2g_set_contract_variant", "giem2g_kernel_launch_count",
+    "giem2g_apply_ie_operator_device_static", "giem2g_batch_create", "giem2g_batch_solve_device",
+    "giem2g_solve_batched", "giem2g_batch_misfit_history", "giem2g_batch_delete",
+    "giem2g_apply_ie_operator_device_batch",
 ]
 
 
@@ -120,6 +123,16 @@ def lib():
     L.giem2g_contract_variants.argtypes = [vp, ip]
     L.giem2g_kernel_launch_count.restype = ctypes.c_longlong
     L.giem2g_set_contract_variant.argtypes = [vp, ip, ip]
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    L.giem2g_apply_ie_operator_device_static.argtypes = [vp, vp, vp, ip]
+    L.giem2g_batch_create.argtypes = [pp, ip, FgmresCtl]
+    L.giem2g_batch_create.restype = vp
+    L.giem2g_batch_solve_device.argtypes = [vp, pp, pp, pp, FgmresCtl, ctypes.POINTER(ResultT)]
+    L.giem2g_solve_batched.argtypes = [vp, pp, pp, pp, FgmresCtl, ctypes.POINTER(ResultT)]
+    L.giem2g_batch_misfit_history.argtypes = [vp, ip, vp, ip]
+    L.giem2g_batch_delete.argtypes = [vp]
+    L.giem2g_batch_delete.restype = None
+    L.giem2g_apply_ie_operator_device_batch.argtypes = [vp, ip, pp, pp, ip]
     _lib = L
     return L
 
@@ -312,3 +325,78 @@ class IEOperator:
             self.delete()
         except Exception:
             pass
+
+
+def _ptrs(xs):
+    arr = (ctypes.c_void_p * len(xs))()
+    for i, x in enumerate(xs):
+        arr[i] = x
+    return arr
+
+
+class Batch:
+    """Several independent solves advanced in lockstep (giem2g_batch_*).
+
+    `ops` lists one IEOperator per instance; an operator may appear twice in a row for the two
+    polarisations of one frequency (their complex64 applies then share tensor reads).
+    """
+
+    def __init__(self, ops, outer_buf=30, inner_buf=10, precision=1, max_restart=100):
+        self.ops = list(ops)
+        self.n = len(self.ops)
+        self._ctl_args = (max_restart, outer_buf, inner_buf, precision)
+        ctl = self.ops[0]._ctl(1e-6, max_restart, outer_buf, inner_buf, precision)
+        self.handle = lib().giem2g_batch_create(_ptrs([o.handle for o in self.ops]), self.n, ctl)
+        if not self.handle:
+            _check(what="giem2g_batch_create")
+
+    def _ctl(self, tol):
+        mr, ob, ib, pr = self._ctl_args
+        return self.ops[0]._ctl(tol, mr, ob, ib, pr)
+
+    def solve_device(self, d_ebkg, d_esol, d_e0=None, tol=1e-6):
+        """Device pointers (lists of ints); returns a list of SolveInfo."""
+        res = (ResultT * self.n)()
+        e0 = _ptrs(d_e0) if d_e0 is not None else None
+        rc = lib().giem2g_batch_solve_device(self.handle, _ptrs(d_ebkg), _ptrs(d_esol), e0, self._ctl(tol), res)
+        _check(rc, "giem2g_batch_solve_device")
+        return [self._info(i, res[i]) for i in range(self.n)]
+
+    def solve(self, E_bkg, E0=None, tol=1e-6):
+        """Host arrays (complex128, (3,Nz,Ny,Nx) each); returns (list of solutions, list of SolveInfo)."""
+        ins = [_c128(e) for e in E_bkg]
+        outs = [np.empty_like(e) for e in ins]
+        e0 = [_c128(e) for e in E0] if E0 is not None else None
+        res = (ResultT * self.n)()
+        rc = lib().giem2g_solve_batched(self.handle, _ptrs([a.ctypes.data for a in ins]),
+                                        _ptrs([a.ctypes.data for a in outs]),
+                                        _ptrs([a.ctypes.data for a in e0]) if e0 is not None else None,
+                                        self._ctl(tol), res)
+        _check(rc, "giem2g_solve_batched")
+        return outs, [self._info(i, res[i]) for i in range(self.n)]
+
+    def _info(self, i, r):
+        return SolveInfo(r.iterations, r.bea, r.be, r.stat, r.applies_fp64, r.applies_fp32, r.device_ms,
+                         self.history(i))
+
+    def history(self, i, max_len=4096):
+        out = np.zeros(max_len)
+        m = lib().giem2g_batch_misfit_history(self.handle, i, out.ctypes.data, max_len)
+        return out[:m]
+
+    def delete(self):
+        if self.handle:
+            lib().giem2g_batch_delete(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass
+
+
+def apply_device_batch(op, d_in, d_out, precision=1):
+    """giem2g_apply_ie_operator_device_batch over lists of device pointers."""
+    _check(lib().giem2g_apply_ie_operator_device_batch(op.handle, len(d_in), _ptrs(d_in), _ptrs(d_out), precision),
+           "apply_device_batch")

@@ -25,6 +25,14 @@ template <typename R> using CT = typename Cplx<R>::T;
 
 constexpr int kThreads = 256;
 
+// The vectors of one apply: nv = 1, or nv = 2 right-hand sides of the same operator that share every
+// tensor read.  Line zc of a pass runs over [0, nv*3Nz): vector zc / 3Nz, row zc % 3Nz.
+template <typename C> struct VecSet {
+    const C *in[2];
+    C *out[2];
+    int nv;
+};
+
 // slot helpers: (kx-pair q, slot bit) and (ky-pair r, mirror bit) of a spectral index
 G2_D void kx_to_slot(int kx, int Nx, int &q, int &sx)
 {
@@ -49,7 +57,7 @@ G2_D void load_tw(C *dst, const C *__restrict__ src, int L)
 // k_fx: pre-scale by gsig, zero-pad to 2Nx, forward x-FFT.  CTA = one y row x NL (z,c) lines.
 // apply_ie_operator_module.F90:57-115 + Distributed_FFT.F90:552-569
 template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_fx(const CT<R> *__restrict__ vin, const CT<R> *__restrict__ gsig,
+__global__ void __launch_bounds__(kThreads) k_fx(const VecSet<CT<R>> vs, const CT<R> *__restrict__ gsig,
                                                  CT<R> *__restrict__ U1, const CT<R> *__restrict__ twg, int Nx,
                                                  int Ny, int Nz, int NL, const int *gate)
 {
@@ -59,16 +67,16 @@ __global__ void __launch_bounds__(kThreads) k_fx(const CT<R> *__restrict__ vin, 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *sm = tw + L;
-    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, y = blockIdx.y;
-    const int nl = min(NL, Z3 - zc0);
+    const int Z3 = 3 * Nz, ZL = vs.nv * Z3, zc0 = blockIdx.x * NL, y = blockIdx.y;
+    const int nl = min(NL, ZL - zc0);
     const size_t plane = (size_t)Nx * Ny;
     load_tw(tw, twg, L);
     __syncthreads();
     auto load = [&](int t, int x) -> C {
-        const int zc = zc0 + t, z = zc % Nz;
-        return cmul(vin[(size_t)zc * plane + (size_t)y * Nx + x], gsig[(size_t)z * plane + (size_t)y * Nx + x]);
+        const int zc = zc0 + t, v = zc >= Z3 ? 1 : 0, lzc = zc - v * Z3, z = lzc % Nz;
+        return cmul(vs.in[v][(size_t)lzc * plane + (size_t)y * Nx + x], gsig[(size_t)z * plane + (size_t)y * Nx + x]);
     };
-    auto store = [&](int t, int kx, C v) { U1[((size_t)kx * Ny + y) * Z3 + zc0 + t] = v; };
+    auto store = [&](int t, int kx, C v) { U1[((size_t)kx * Ny + y) * ZL + zc0 + t] = v; };
     auto off = [&](int t, int n1, int k2) { return n1 + N1 * k2 + (L + 1) * t; };
     fft4step<C, N1, N2, false, true, false, false, true>(sm, nl, tw, load, store, off);
 }
@@ -78,7 +86,7 @@ __global__ void __launch_bounds__(kThreads) k_fx(const CT<R> *__restrict__ vin, 
 template <typename R, int L>
 __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uh,
                                                  const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
-                                                 const int *gate)
+                                                 int nv, const int *gate)
 {
     if (gate && *gate == 0) return;
     using C = CT<R>;
@@ -86,7 +94,7 @@ __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, C
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *sm = tw + L;
-    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, kx = blockIdx.y;
+    const int Z3 = nv * 3 * Nz, zc0 = blockIdx.x * NL, kx = blockIdx.y;  // Z3: lines of all vectors
     const int nl = min(NL, Z3 - zc0);
     int q, sx;
     kx_to_slot(kx, Nx, q, sx);
@@ -115,7 +123,7 @@ __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, C
 template <typename R, int L>
 __global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, CT<R> *__restrict__ U1,
                                                  const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
-                                                 const int *gate)
+                                                 int nv, const int *gate)
 {
     if (gate && *gate == 0) return;
     using C = CT<R>;
@@ -123,7 +131,7 @@ __global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, C
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *sm = tw + L;
-    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, kx = blockIdx.y;
+    const int Z3 = nv * 3 * Nz, zc0 = blockIdx.x * NL, kx = blockIdx.y;  // Z3: lines of all vectors
     if (kx == Nx) return;  // x-Nyquist column is read as zero by k_bx
     const int nl = min(NL, Z3 - zc0);
     int q, sx;
@@ -143,10 +151,10 @@ __global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, C
 // k_bx: inverse x-FFT, crop x < Nx, post-combine y = s*(a*x - w/(dz*4NxNy)).
 // apply_ie_operator_module.F90:125-174
 template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, const CT<R> *__restrict__ vin,
+__global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, const VecSet<CT<R>> vs,
                                                  const CT<R> *__restrict__ asig, const R *__restrict__ post,
-                                                 CT<R> *__restrict__ vout, const CT<R> *__restrict__ twg, int Nx,
-                                                 int Ny, int Nz, int NL, const int *gate)
+                                                 const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
+                                                 const int *gate)
 {
     if (gate && *gate == 0) return;
     using C = CT<R>;
@@ -154,24 +162,24 @@ __global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, c
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *sm = tw + L;
-    const int Z3 = 3 * Nz, zc0 = blockIdx.x * NL, y = blockIdx.y;
-    const int nl = min(NL, Z3 - zc0);
+    const int Z3 = 3 * Nz, ZL = vs.nv * Z3, zc0 = blockIdx.x * NL, y = blockIdx.y;
+    const int nl = min(NL, ZL - zc0);
     const size_t plane = (size_t)Nx * Ny;
     load_tw(tw, twg, L);
     __syncthreads();
     auto load = [&](int t, int kx) -> C {
-        return kx == Nx ? czero<C>() : U1[((size_t)kx * Ny + y) * Z3 + zc0 + t];
+        return kx == Nx ? czero<C>() : U1[((size_t)kx * Ny + y) * ZL + zc0 + t];
     };
     auto store = [&](int t, int x, C w) {
-        const int zc = zc0 + t, z = zc % Nz;
+        const int zc = zc0 + t, v = zc >= Z3 ? 1 : 0, lzc = zc - v * Z3, z = lzc % Nz;
         const size_t cell = (size_t)z * plane + (size_t)y * Nx + x;
-        const size_t idx = (size_t)zc * plane + (size_t)y * Nx + x;
-        const C d1 = cmul(vin[idx], asig[cell]);
+        const size_t idx = (size_t)lzc * plane + (size_t)y * Nx + x;
+        const C d1 = cmul(vs.in[v][idx], asig[cell]);
         const R sq = post[z], inv = post[Nz + z];
         C o;
         o.x = (d1.x - w.x * inv) * sq;
         o.y = (d1.y - w.y * inv) * sq;
-        vout[idx] = o;
+        vs.out[v][idx] = o;
     };
     auto off = [&](int t, int n1, int k2) { return t * (L + 1) + k2 + N2 * n1; };
     fft4step<C, N1, N2, true, false, true, true, false>(sm, nl, tw, load, store, off);
@@ -328,65 +336,64 @@ template <typename K> static void big_smem(K k)
 }
 
 template <typename R, int L>
-static void launch_x(bool fwd, IeOp *op, const CT<R> *d_in, CT<R> *d_out, CT<R> *U1, cudaStream_t st,
-                     const int *gate)
+static void launch_x(bool fwd, IeOp *op, const VecSet<CT<R>> &vs, CT<R> *U1, cudaStream_t st, const int *gate)
 {
-    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = vs.nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
     const int NL = lines_for(L, es), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
-    dim3 grid((Z3 + NL - 1) / NL, Ny);
+    dim3 grid((ZL + NL - 1) / NL, Ny);
     static bool attr = false;
     if (!attr) { big_smem(k_fx<R, L>); big_smem(k_bx<R, L>); attr = true; }
     if (fwd)
-        k_fx<R, L><<<grid, nt, sm, st>>>(d_in, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
+        k_fx<R, L><<<grid, nt, sm, st>>>(vs, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
     else
-        k_bx<R, L><<<grid, nt, sm, st>>>(U1, d_in, Bufs<R>::asig(op), Bufs<R>::post(op), d_out,
-                                         Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
+        k_bx<R, L><<<grid, nt, sm, st>>>(U1, vs, Bufs<R>::asig(op), Bufs<R>::post(op), Bufs<R>::twx(op), Nx, Ny,
+                                         Nz, NL, gate);
 }
 
 template <typename R, int L>
-static void launch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
+static void launch_y(bool fwd, IeOp *op, int nv, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
 {
-    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, Z3 = 3 * Nz;
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
     const int NL = lines_for(L, es), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
-    dim3 grid((Z3 + NL - 1) / NL, 2 * Nx);
+    dim3 grid((ZL + NL - 1) / NL, 2 * Nx);
     static bool attr = false;
     if (!attr) { big_smem(k_fy<R, L>); big_smem(k_by<R, L>); attr = true; }
-    if (fwd) k_fy<R, L><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL, gate);
-    else k_by<R, L><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL, gate);
+    if (fwd) k_fy<R, L><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL, nv, gate);
+    else k_by<R, L><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL, nv, gate);
 }
 
 template <typename R>
-static void dispatch_x(bool fwd, IeOp *op, const CT<R> *i, CT<R> *o, CT<R> *U1, cudaStream_t st, const int *gate)
+static void dispatch_x(bool fwd, IeOp *op, const VecSet<CT<R>> &vs, CT<R> *U1, cudaStream_t st, const int *gate)
 {
     switch (2 * op->Nx) {
-    case 4: launch_x<R, 4>(fwd, op, i, o, U1, st, gate); break;
-    case 8: launch_x<R, 8>(fwd, op, i, o, U1, st, gate); break;
-    case 16: launch_x<R, 16>(fwd, op, i, o, U1, st, gate); break;
-    case 32: launch_x<R, 32>(fwd, op, i, o, U1, st, gate); break;
-    case 64: launch_x<R, 64>(fwd, op, i, o, U1, st, gate); break;
-    case 128: launch_x<R, 128>(fwd, op, i, o, U1, st, gate); break;
-    case 256: launch_x<R, 256>(fwd, op, i, o, U1, st, gate); break;
-    case 512: launch_x<R, 512>(fwd, op, i, o, U1, st, gate); break;
-    case 1024: launch_x<R, 1024>(fwd, op, i, o, U1, st, gate); break;
+    case 4: launch_x<R, 4>(fwd, op, vs, U1, st, gate); break;
+    case 8: launch_x<R, 8>(fwd, op, vs, U1, st, gate); break;
+    case 16: launch_x<R, 16>(fwd, op, vs, U1, st, gate); break;
+    case 32: launch_x<R, 32>(fwd, op, vs, U1, st, gate); break;
+    case 64: launch_x<R, 64>(fwd, op, vs, U1, st, gate); break;
+    case 128: launch_x<R, 128>(fwd, op, vs, U1, st, gate); break;
+    case 256: launch_x<R, 256>(fwd, op, vs, U1, st, gate); break;
+    case 512: launch_x<R, 512>(fwd, op, vs, U1, st, gate); break;
+    case 1024: launch_x<R, 1024>(fwd, op, vs, U1, st, gate); break;
     }
 }
 template <typename R>
-static void dispatch_y(bool fwd, IeOp *op, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
+static void dispatch_y(bool fwd, IeOp *op, int nv, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
 {
     switch (2 * op->Ny) {
-    case 4: launch_y<R, 4>(fwd, op, U1, Uh, st, gate); break;
-    case 8: launch_y<R, 8>(fwd, op, U1, Uh, st, gate); break;
-    case 16: launch_y<R, 16>(fwd, op, U1, Uh, st, gate); break;
-    case 32: launch_y<R, 32>(fwd, op, U1, Uh, st, gate); break;
-    case 64: launch_y<R, 64>(fwd, op, U1, Uh, st, gate); break;
-    case 128: launch_y<R, 128>(fwd, op, U1, Uh, st, gate); break;
-    case 256: launch_y<R, 256>(fwd, op, U1, Uh, st, gate); break;
-    case 512: launch_y<R, 512>(fwd, op, U1, Uh, st, gate); break;
-    case 1024: launch_y<R, 1024>(fwd, op, U1, Uh, st, gate); break;
+    case 4: launch_y<R, 4>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 8: launch_y<R, 8>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 16: launch_y<R, 16>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 32: launch_y<R, 32>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 64: launch_y<R, 64>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 128: launch_y<R, 128>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 256: launch_y<R, 256>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 512: launch_y<R, 512>(fwd, op, nv, U1, Uh, st, gate); break;
+    case 1024: launch_y<R, 1024>(fwd, op, nv, U1, Uh, st, gate); break;
     }
 }
 
@@ -400,8 +407,9 @@ static int ie_apply_core(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t
     const size_t es = sizeof(CT<R>);
     const CT<R> *G = Bufs<R>::G(op);
     if (!G || !U1 || !Uh) return G2_ERR_STATE;
-    dispatch_x<R>(true, op, d_in, nullptr, U1, st, gate);
-    dispatch_y<R>(true, op, U1, Uh, st, gate);
+    VecSet<CT<R>> vs{{d_in, nullptr}, {d_out, nullptr}, 1};
+    dispatch_x<R>(true, op, vs, U1, st, gate);
+    dispatch_y<R>(true, op, 1, U1, Uh, st, gate);
     // contraction
     int rc_fast = G2_ERR_UNSUPPORTED;
     if (op->use_fast_contract) {
@@ -419,8 +427,8 @@ static int ie_apply_core(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t
         const int threads = ((Z3 + 31) / 32) * 32;
         k_contract<R><<<(unsigned)op->units(), threads, sm, st>>>(G, Uh, Nx, Ny, Nz, gate);
     }
-    dispatch_y<R>(false, op, U1, Uh, st, gate);
-    dispatch_x<R>(false, op, d_in, d_out, U1, st, gate);
+    dispatch_y<R>(false, op, 1, U1, Uh, st, gate);
+    dispatch_x<R>(false, op, vs, U1, st, gate);
     g2_count_launches(5);
     G2_CUDA_CHECK(cudaGetLastError());
     return G2_OK;
@@ -540,5 +548,42 @@ int ie_prepare_sigma(IeOp *op, cudaStream_t st)
     G2_CUDA_CHECK(cudaStreamSynchronize(st));
     cudaFree(d_csigb);
     cudaFree(d_sq);
+    return G2_OK;
+}
+
+size_t ie_pair_scratch_elems(const IeOp *op, size_t *n_u1)
+{
+    size_t u1 = 0;
+    const size_t all = ie_apply_scratch_elems(op, &u1);
+    if (n_u1) *n_u1 = 2 * u1;
+    return 2 * all;
+}
+// Two complex64 vectors of one operator in one apply: the FFT passes run over both vectors' lines and the
+// contraction applies each tensor unit, read once, to both spectra.  Returns G2_ERR_UNSUPPORTED (nothing
+// launched) when no paired contraction exists for the grid.
+int ie_apply_pair32(IeOp *op, const float2 *in0, const float2 *in1, float2 *out0, float2 *out1, cudaStream_t st,
+                    float2 *U1, float2 *Uh)
+{
+    if (!op->use_fast_contract || !ie_contract_pair32_supported(op->Nx, op->Ny, op->Nz)) return G2_ERR_UNSUPPORTED;
+    if (!op->d_tensor32 || !U1 || !Uh) return G2_ERR_STATE;
+    VecSet<float2> vs{{in0, in1}, {out0, out1}, 2};
+    dispatch_x<float>(true, op, vs, U1, st, nullptr);
+    dispatch_y<float>(true, op, 2, U1, Uh, st, nullptr);
+    const int rc = ie_contract_pair32(op->d_tensor32, Uh, op->Nx, op->Ny, op->Nz, op->d_err, st, nullptr);
+    if (rc) return rc;
+    dispatch_y<float>(false, op, 2, U1, Uh, st, nullptr);
+    dispatch_x<float>(false, op, vs, U1, st, nullptr);
+    g2_count_launches(5);
+    G2_CUDA_CHECK(cudaGetLastError());
+    return G2_OK;
+}
+int ie_pair_scratch(IeOp *op, float2 **U1, float2 **Uh)
+{
+    size_t n_u1 = 0;
+    const size_t n_all = ie_pair_scratch_elems(op, &n_u1);
+    if (!op->pair_scratch.U1) G2_CUDA_CHECK(cudaMalloc(&op->pair_scratch.U1, n_u1 * sizeof(float2)));
+    if (!op->pair_scratch.Uhat) G2_CUDA_CHECK(cudaMalloc(&op->pair_scratch.Uhat, (n_all - n_u1) * sizeof(float2)));
+    *U1 = reinterpret_cast<float2 *>(op->pair_scratch.U1);
+    *Uh = reinterpret_cast<float2 *>(op->pair_scratch.Uhat);
     return G2_OK;
 }

@@ -436,6 +436,116 @@ int giem2g_solve(void *ie, const void *E_bkg, void *Esol, const void *E0, GIEM2G
     return set_status(0);
 }
 
+void *giem2g_batch_create(void *const *ies, int n, GIEM2G_FGMRES_CTL ctl)
+{
+    if (!ies || n < 1) { fail(G2_ERR_ARG, "giem2g_batch_create: no operators"); return nullptr; }
+    std::vector<IeOp *> ops(n);
+    for (int i = 0; i < n; i++) {
+        ops[i] = resolve(ies[i]);
+        if (check_ready(ops[i], "giem2g_batch_create")) return nullptr;
+    }
+    void *b = nullptr;
+    const int rc = batch_create(ops.data(), n, ctl.fgmres_buf, ctl.gmres_buf, ctl.precision, &b);
+    if (rc) { fail(rc, "giem2g_batch_create: %s", giem2g_last_error()); return nullptr; }
+    set_status(0);
+    return b;
+}
+
+int giem2g_batch_solve_device(void *batch, const void *const *d_Ebkg, void *const *d_Esol, const void *const *d_E0,
+                              GIEM2G_FGMRES_CTL ctl, GIEM2G_RESULT *info)
+{
+    if (!batch || !d_Ebkg || !d_Esol || !info) return fail(G2_ERR_ARG, "giem2g_batch_solve_device: NULL argument");
+    const int rc = batch_solve_device(batch, reinterpret_cast<const double2 *const *>(d_Ebkg),
+                                      reinterpret_cast<double2 *const *>(d_Esol),
+                                      reinterpret_cast<const double2 *const *>(d_E0), ctl, info);
+    if (rc) return fail(rc, "giem2g_batch_solve_device: %s", giem2g_last_error());
+    return set_status(0);
+}
+
+int giem2g_solve_batched(void *batch, const void *const *E_bkg, void *const *Esol, const void *const *E0,
+                         GIEM2G_FGMRES_CTL ctl, GIEM2G_RESULT *info)
+{
+    // host arrays: every E_bkg[i] (and E0[i]) is copied in, every Esol[i] copied out
+    if (!batch || !E_bkg || !Esol || !info) return fail(G2_ERR_ARG, "giem2g_solve_batched: NULL argument");
+    double2 *stage = nullptr;
+    size_t N = 0;
+    int rc = batch_stage(batch, &stage, &N);
+    if (rc) return fail(rc, "giem2g_solve_batched: %s", giem2g_last_error());
+    const int n = batch_size(batch);
+    cudaStream_t st = batch_op(batch, 0)->stream;
+    std::vector<const double2 *> in(n), e0(n, nullptr);
+    std::vector<double2 *> out(n);
+    for (int i = 0; i < n; i++) {
+        const size_t nb = batch_op(batch, i)->nvec() * sizeof(double2);
+        in[i] = stage + (size_t)i * N;
+        out[i] = stage + (size_t)(n + i) * N;
+        if (cudaMemcpyAsync(const_cast<double2 *>(in[i]), E_bkg[i], nb, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return fail(G2_ERR_CUDA, "giem2g_solve_batched: copy failed");
+        if (E0 && E0[i]) {
+            e0[i] = stage + (size_t)(2 * n + i) * N;
+            if (cudaMemcpyAsync(const_cast<double2 *>(e0[i]), E0[i], nb, cudaMemcpyHostToDevice, st) != cudaSuccess)
+                return fail(G2_ERR_CUDA, "giem2g_solve_batched: copy failed");
+        }
+    }
+    rc = batch_solve_device(batch, in.data(), out.data(), e0.data(), ctl, info);
+    if (rc) return fail(rc, "giem2g_solve_batched: %s", giem2g_last_error());
+    for (int i = 0; i < n; i++) {
+        if (cudaMemcpyAsync(Esol[i], out[i], batch_op(batch, i)->nvec() * sizeof(double2), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess)
+            return fail(G2_ERR_CUDA, "giem2g_solve_batched: copy back failed");
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(G2_ERR_CUDA, "giem2g_solve_batched: sync failed");
+    return set_status(0);
+}
+
+int giem2g_batch_misfit_history(void *batch, int i, double *out, int max_len)
+{
+    if (!batch || !out) return 0;
+    return batch_history(batch, i, out, max_len);
+}
+
+void giem2g_batch_delete(void *batch)
+{
+    batch_free(batch);
+    set_status(0);
+}
+
+int giem2g_apply_ie_operator_device_batch(void *ie, int nv, const void *const *d_in, void *const *d_out, int precision)
+{
+    IeOp *op = resolve(ie);
+    int rc = check_ready(op, "giem2g_apply_ie_operator_device_batch");
+    if (rc) return rc;
+    if (nv < 1 || !d_in || !d_out || (precision != 0 && precision != 1))
+        return fail(G2_ERR_ARG, "giem2g_apply_ie_operator_device_batch: bad arguments");
+    cudaEventRecord(op->ev0, op->stream);
+    int i = 0;
+    if (precision == 1) {
+        float2 *U1 = nullptr, *Uh = nullptr;
+        for (; i + 1 < nv; i += 2) {
+            if (!U1 && (rc = ie_pair_scratch(op, &U1, &Uh)))
+                return fail(rc, "giem2g_apply_ie_operator_device_batch: %s", giem2g_last_error());
+            rc = ie_apply_pair32(op, reinterpret_cast<const float2 *>(d_in[i]), reinterpret_cast<const float2 *>(d_in[i + 1]),
+                                 reinterpret_cast<float2 *>(d_out[i]), reinterpret_cast<float2 *>(d_out[i + 1]), op->stream,
+                                 U1, Uh);
+            if (rc == G2_ERR_UNSUPPORTED) break;
+            if (rc) return fail(rc, "giem2g_apply_ie_operator_device_batch: %s", giem2g_last_error());
+            op->mult_num += 2;
+        }
+    }
+    for (; i < nv; i++) {
+        if (precision == 0)
+            rc = ie_apply_device64(op, reinterpret_cast<const double2 *>(d_in[i]), reinterpret_cast<double2 *>(d_out[i]),
+                                   op->stream);
+        else
+            rc = ie_apply_device32(op, reinterpret_cast<const float2 *>(d_in[i]), reinterpret_cast<float2 *>(d_out[i]),
+                                   op->stream);
+        if (rc) return fail(rc, "giem2g_apply_ie_operator_device_batch: %s", giem2g_last_error());
+        op->mult_num++;
+    }
+    cudaEventRecord(op->ev1, op->stream);
+    return set_status(0);
+}
+
 int giem2g_get_misfit_history(void *ie, double *out, int max_len)
 {
     IeOp *op = resolve(ie);
@@ -494,7 +604,8 @@ void giem2g_delete_ie_operator(void *ie)
     krylov_free(op);
     void *ptrs[] = {op->d_spatial, op->d_tensor64, op->d_tensor32, op->d_csiga, op->d_gsig64, op->d_asig64,
                     op->d_gsig32, op->d_asig32, op->d_post64, op->d_post32, op->d_twx64, op->d_twy64,
-                    op->d_twx32, op->d_twy32, op->scratch.U1, op->scratch.Uhat, op->d_vin, op->d_vout, op->d_err};
+                    op->d_twx32, op->d_twy32, op->scratch.U1, op->scratch.Uhat, op->pair_scratch.U1,
+                    op->pair_scratch.Uhat, op->d_vin, op->d_vout, op->d_err};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (op->ev0) cudaEventDestroy(op->ev0);

@@ -24,19 +24,20 @@
 
 namespace {
 
-template <typename R, int NZ, int S, int B, int NSTAGE>
+template <typename R, int NZ, int S, int B, int NSTAGE, int NP = 1>
 struct CfgT {
     static constexpr int P = NZ * (NZ + 1) / 2;
     static constexpr int T = 4 * P + 2 * NZ * NZ;        // complex per unit
     static constexpr int Z3 = 3 * NZ;
+    static constexpr int PTS = 4 * NP;                     // spectral points per unit: 4 slots x NP vectors
     static constexpr int NC = B * S * NZ;                  // consumer threads
     static constexpr int NTHREADS = NC + 32;
     static constexpr int JS = NZ / S;                      // j per slice
     static constexpr int ES = 2 * sizeof(R);               // bytes per complex
     static constexpr int TBYTES = B * T * ES;
-    static constexpr int UBYTES = B * 4 * Z3 * ES;
+    static constexpr int UBYTES = B * PTS * Z3 * ES;
     static constexpr int STAGE_BYTES = TBYTES + UBYTES;
-    static constexpr int RED_BYTES = S * B * 12 * NZ * ES;
+    static constexpr int RED_BYTES = S * B * PTS * 3 * NZ * ES;
     static constexpr int SMEM = NSTAGE * STAGE_BYTES + 2 * NSTAGE * 8;
     static_assert(NZ % S == 0, "slices must divide Nz");
     static_assert(NC % 32 == 0, "consumer threads must be whole warps");
@@ -52,13 +53,16 @@ template <> struct V2<float> { using T = float2; };
 template <int NZ>
 G2_D int sym_idx(int i, int j) { return i <= j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2; }
 
-template <typename R, int NZ, int S, int B, int NSTAGE>
-__global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
+// NP > 1: NP vectors share every tensor unit (several right-hand sides of one operator); the spectrum of
+// a unit is [slot][vector][3Nz] and point pt = slot * NP + vector.
+template <typename R, int NZ, int S, int B, int NSTAGE, int NP>
+__global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP>::NTHREADS, 1)
     k_contract_tma(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
                    long long nbatches, int *err, const int *gate)
 {
     if (gate && *gate == 0) return;  // uniform across the CTA: nothing has been issued yet
-    using Cfg = CfgT<R, NZ, S, B, NSTAGE>;
+    using Cfg = CfgT<R, NZ, S, B, NSTAGE, NP>;
+    constexpr int PTS = Cfg::PTS;
     using C2 = typename V2<R>::T;
     constexpr int AW = sizeof(R) == 8 ? asw_width64(NZ) : asw_width32(NZ);
     extern __shared__ __align__(128) unsigned char smem[];
@@ -96,7 +100,7 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
                 unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
                 mbar_arrive_expect_tx(&full[slot], Cfg::STAGE_BYTES);
                 bulk_g2s(st, G + batch * (long long)B * Cfg::T, Cfg::TBYTES, &full[slot], pol_t);
-                bulk_g2s(st + Cfg::TBYTES, Uhat + batch * (long long)B * 4 * Cfg::Z3, Cfg::UBYTES, &full[slot], pol_u);
+                bulk_g2s(st + Cfg::TBYTES, Uhat + batch * (long long)B * PTS * Cfg::Z3, Cfg::UBYTES, &full[slot], pol_u);
                 issued++;
             }
             if (!ok) {
@@ -120,41 +124,41 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
         unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
         const C2 *gt = reinterpret_cast<const C2 *>(st);
         const C2 *uh = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);
-        R acc[3][4][3];
+        R acc[3][PTS][3];
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
-            for (int p = 0; p < 4; p++)
+            for (int p = 0; p < PTS; p++)
 #pragma unroll
                 for (int k = 0; k < 3; k++) acc[c][p][k] = R(0);
 
         const C2 *gb = gt + b * Cfg::T;
         const C2 *gxx = gb, *gxy = gb + Cfg::P, *gyy = gb + 2 * Cfg::P, *gzz = gb + 3 * Cfg::P;
         const C2 *gxz = gb + 4 * Cfg::P, *gyz = gb + 4 * Cfg::P + NZ * NZ;
-        const C2 *ub = uh + b * 4 * Cfg::Z3;  // [p][c][j], broadcast reads
+        const C2 *ub = uh + b * PTS * Cfg::Z3;  // [pt][c][j], broadcast reads
 #pragma unroll 2
         for (int jj = 0; jj < Cfg::JS; jj++) {
             const int j = s * Cfg::JS + jj;
             const int si = sym_idx<NZ>(z, j);
             const int a_zj = asw(z, j, NZ, AW), a_jz = asw(j, z, NZ, AW);
             const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[a_zj], gyz[a_zj], gxz[a_jz], gyz[a_jz]};
-            C2 u[4][3];
-            R ue[4][3];
+            C2 u[PTS][3];
+            R ue[PTS][3];
 #pragma unroll
-            for (int p = 0; p < 4; p++)
+            for (int p = 0; p < PTS; p++)
 #pragma unroll
                 for (int c = 0; c < 3; c++) {
                     u[p][c] = ub[(p * 3 + c) * NZ + j];
                     ue[p][c] = u[p][c].x + u[p][c].y;
                 }
-            // term-major: each term updates 12 independent accumulators (4 points x 3 partial products)
+            // term-major: each term updates 3*PTS independent accumulators (PTS points x 3 partial products)
 #define G2_TERM(C, K, IN, SGN)                                                   \
     {                                                                            \
         const R es_ = e[K].x + e[K].y;                                           \
-        _Pragma("unroll") for (int p = 0; p < 4; p++)                            \
+        _Pragma("unroll") for (int p = 0; p < PTS; p++)                          \
         {                                                                        \
-            const R sx = (p & 2) ? R(-1) : R(1);                                 \
-            const R m = (p & 1) ? R(-1) : R(1);                                  \
+            const R sx = ((p / NP) & 2) ? R(-1) : R(1);                          \
+            const R m = ((p / NP) & 1) ? R(-1) : R(1);                           \
             const R sg = (SGN);                                                  \
             acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);           \
             acc[C][p][1] = fma(sg * e[K].y, u[p][IN].y, acc[C][p][1]);           \
@@ -176,43 +180,43 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE>::NTHREADS, 1)
 #undef G2_TERM
         }
         named_bar_sync(1, Cfg::NC);  // all reads of this stage's tensor and inputs are done
-        // slice partials into the drained tensor area: red[s][b][p][c][z]
+        // slice partials into the drained tensor area: red[s][b][pt][c][z]
         C2 *red = reinterpret_cast<C2 *>(st);
 #pragma unroll
-        for (int p = 0; p < 4; p++)
+        for (int p = 0; p < PTS; p++)
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const R t1 = acc[c][p][0], t2 = acc[c][p][1], t3 = acc[c][p][2];
                 C2 v;
                 v.x = t1 - t2;
                 v.y = t3 - t1 - t2;
-                red[(((s * B + b) * 4 + p) * 3 + c) * NZ + z] = v;
+                red[(((s * B + b) * PTS + p) * 3 + c) * NZ + z] = v;
             }
         named_bar_sync(1, Cfg::NC);
-        for (int o = tid; o < B * 12 * NZ; o += Cfg::NC) {
-            const int bb = o / (12 * NZ), rem = o - bb * 12 * NZ, p = rem / (3 * NZ);
-            C2 v = red[bb * 12 * NZ + rem];
+        for (int o = tid; o < B * PTS * 3 * NZ; o += Cfg::NC) {
+            const int bb = o / (PTS * 3 * NZ), rem = o - bb * PTS * 3 * NZ, p = rem / (3 * NZ) / NP;
+            C2 v = red[bb * PTS * 3 * NZ + rem];
 #pragma unroll
             for (int ss = 1; ss < S; ss++) {
-                const C2 w = red[(ss * B + bb) * 12 * NZ + rem];
+                const C2 w = red[(ss * B + bb) * PTS * 3 * NZ + rem];
                 v.x += w.x;
                 v.y += w.y;
             }
             const long long unit = batch * B + bb;
             const int q = (int)(unit / Ny), r = (int)(unit - (long long)q * Ny);
             if ((q == 0 && (p & 2)) || (r == 0 && (p & 1))) { v.x = R(0); v.y = R(0); }
-            Uhat[unit * 4 * Cfg::Z3 + rem] = v;
+            Uhat[unit * PTS * Cfg::Z3 + rem] = v;
         }
         named_bar_sync(1, Cfg::NC);  // red reads done before the slot is refilled
         mbar_arrive(&empty[slot]);
     }
 }
 
-template <typename R, int NZ, int S, int B, int NSTAGE>
+template <typename R, int NZ, int S, int B, int NSTAGE, int NP = 1>
 int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
-    using Cfg = CfgT<R, NZ, S, B, NSTAGE>;
-    auto kern = k_contract_tma<R, NZ, S, B, NSTAGE>;
+    using Cfg = CfgT<R, NZ, S, B, NSTAGE, NP>;
+    auto kern = k_contract_tma<R, NZ, S, B, NSTAGE, NP>;
     static bool attr = false;
     if (!attr) {
         G2_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
@@ -276,5 +280,31 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48: return launch_cfg<float, 48, 4, 1, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
+    }
+}
+
+// Two vectors of one operator per tensor read (complex64; both polarisations of a plane-wave source).
+// The spectrum holds [unit][slot][vector][3Nz].
+int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
+                       const int *gate)
+{
+    const int n = sm_count();
+    switch (Nz) {
+    case 8: return launch_cfg<float, 8, 1, 16, 3, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 16: return launch_cfg<float, 16, 2, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 32: return launch_cfg<float, 32, 4, 1, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 48: return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+    default: return G2_ERR_UNSUPPORTED;
+    }
+}
+bool ie_contract_pair32_supported(int Nx, int Ny, int Nz)
+{
+    const long long u = (long long)Nx * Ny;
+    switch (Nz) {
+    case 8: return u % 16 == 0;
+    case 16: return u % 4 == 0;
+    case 32:
+    case 48: return true;
+    default: return false;
     }
 }

@@ -40,6 +40,7 @@ struct IeOp {
     double2 *d_twx64 = nullptr, *d_twy64 = nullptr;
     float2 *d_twx32 = nullptr, *d_twy32 = nullptr;
     ApplyScratch scratch;
+    ApplyScratch pair_scratch;         // two complex64 vectors per apply (allocated on first paired apply)
     int *d_err = nullptr;              // device error word written by bounded waits (0 = ok)
     void *krylov = nullptr;            // solver workspace (krylov.cu)
     // host staging for the reference-facing (host-pointer) apply
@@ -73,6 +74,15 @@ int ie_apply_device64_scratch(IeOp *op, const double2 *d_in, double2 *d_out, cud
                               double2 *Uhat);
 int ie_apply_device32_scratch(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, float2 *U1,
                               float2 *Uhat);
+// Two complex64 vectors of one operator per apply (shared tensor reads); scratch holds twice the
+// single-vector intermediates.  G2_ERR_UNSUPPORTED when the grid has no paired contraction.
+size_t ie_pair_scratch_elems(const IeOp *op, size_t *n_u1);
+int ie_pair_scratch(IeOp *op, float2 **U1, float2 **Uh);
+int ie_apply_pair32(IeOp *op, const float2 *in0, const float2 *in1, float2 *out0, float2 *out1, cudaStream_t st,
+                    float2 *U1, float2 *Uh);
+bool ie_contract_pair32_supported(int Nx, int Ny, int Nz);
+int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
+                       const int *gate);
 // Process-wide static scratch of the static-scratch apply: device address (set-up on first use per
 // device) and capacity in bytes.
 int ie_static_scratch(void **ptr, size_t *capacity);

@@ -477,9 +477,8 @@ static void free_level(Level &L)
     L = Level();
 }
 
-void krylov_free(IeOp *op)
+static void kw_free(KrylovWork *k)
 {
-    KrylovWork *k = reinterpret_cast<KrylovWork *>(op->krylov);
     if (!k) return;
     if (k->inner_exec) cudaGraphExecDestroy(k->inner_exec);
     void *p[] = {k->Vo, k->x, k->b, k->r0, k->w, k->tmp, k->Zo, k->Vi, k->ri, k->wi, k->vin, k->xin, k->part};
@@ -488,21 +487,22 @@ void krylov_free(IeOp *op)
     free_level(k->Lo);
     free_level(k->Li);
     delete k;
+}
+
+void krylov_free(IeOp *op)
+{
+    kw_free(reinterpret_cast<KrylovWork *>(op->krylov));
     op->krylov = nullptr;
 }
 
-static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
+// solver workspace for vectors of N complex: outer basis mo, inner basis mi
+static int kw_alloc(KrylovWork *k, size_t N, int mo, int mi, int precision)
 {
-    KrylovWork *k = reinterpret_cast<KrylovWork *>(op->krylov);
-    if (k && k->mo == mo && k->mi == mi && k->precision == precision) return G2_OK;
-    krylov_free(op);
-    k = new KrylovWork();
-    op->krylov = k;
-    k->N = op->nvec();
+    k->N = N;
     k->mo = mo;
     k->mi = mi;
     k->precision = precision;
-    const size_t N = k->N, e64 = sizeof(double2), ei = precision ? sizeof(float2) : sizeof(double2);
+    const size_t e64 = sizeof(double2), ei = precision ? sizeof(float2) : sizeof(double2);
     G2_CUDA_CHECK(cudaMalloc(&k->Vo, e64 * N * (mo + 1)));
     G2_CUDA_CHECK(cudaMalloc(&k->x, e64 * N));
     G2_CUDA_CHECK(cudaMalloc(&k->b, e64 * N));
@@ -520,6 +520,16 @@ static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
     int rc = alloc_level(k->Lo, mo);
     if (!rc) rc = alloc_level(k->Li, mi);
     return rc;
+}
+
+static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
+{
+    KrylovWork *k = reinterpret_cast<KrylovWork *>(op->krylov);
+    if (k && k->mo == mo && k->mi == mi && k->precision == precision) return G2_OK;
+    krylov_free(op);
+    k = new KrylovWork();
+    op->krylov = k;
+    return kw_alloc(k, op->nvec(), mo, mi, precision);
 }
 
 // ---- launch helpers ------------------------------------------------------------------------------
@@ -865,3 +875,527 @@ int krylov_history(IeOp *op, double *out, int max_len)
     for (int i = 0; i < n; i++) out[i] = k->history[i];
     return n;
 }
+
+// ==================================================================================================
+// Batched solves (several frequencies and both polarisations): n independent instances, each a full
+// nested FGMRES with its own workspace, advanced in lockstep on one stream.  Per outer step the host
+// launches every active instance's work, replays ONE captured inner cycle for all instances and reads
+// all instances' scalars with one synchronisation.  Consecutive instances of the same operator form
+// pairs whose complex64 applies share every tensor read (ie_apply_pair32).  Each instance follows exactly
+// the launch sequence of the single solve, so its iterates, iteration count and status are those of a
+// solve on its own.  Converged instances are masked: their inner-cycle kernels are gated off through a
+// device flag and the host stops launching their outer work.
+namespace {
+
+__global__ void k_set_bn_masked(Level L, const int *active)
+{
+    L.scal[S_BN] = sqrt(L.scal[S_NRM2]);
+    L.flags[F_SOLVER] = (L.scal[S_BN] < ZERO_THRESHOLD || *active == 0) ? 0 : 1;
+    L.flags[F_ITER] = 0;
+    L.flags[F_KRYLOV] = L.flags[F_SOLVER];
+    L.flags[F_L] = 0;
+    L.flags[F_PASS] = 0;
+}
+
+}  // namespace
+
+struct BatchGroup {
+    IeOp *op = nullptr;
+    int first = 0, n = 0;  // instances first .. first+n-1 (n = 1 or 2)
+};
+
+struct BatchWork {
+    int n = 0, mo = 0, mi = 0, precision = -1;
+    std::vector<IeOp *> ops;
+    std::vector<KrylovWork *> k;
+    std::vector<BatchGroup> groups;
+    int *d_active = nullptr;
+    std::vector<int> h_active, dev_active;
+    double2 *d_stage = nullptr;  // host-array solves: E_bkg[n] then E_sol[n] (complex128)
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t inner_exec = nullptr;
+    double inner_tol = -1.0;
+    int inner_uses = 0, inner_graph_launches = 0;
+    std::vector<int> inner_graph_applies, cv;
+    std::vector<std::vector<double>> history;
+};
+
+static void batch_destroy(BatchWork *b)
+{
+    if (!b) return;
+    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->inner_exec) cudaGraphExecDestroy(b->inner_exec);
+    for (KrylovWork *k : b->k) kw_free(k);
+    if (b->d_active) cudaFree(b->d_active);
+    if (b->d_stage) cudaFree(b->d_stage);
+    delete b;
+}
+
+int batch_create(IeOp *const *ops, int n, int mo, int mi, int precision, void **out)
+{
+    *out = nullptr;
+    if (n < 1) return G2_ERR_ARG;
+    if (mo < 1 || mi < 1 || mo > KMAX - 1 || mi > KMAX - 1) {
+        g2_set_error_msg("FGMRES buffer sizes must be in [1, 31]");
+        return G2_ERR_UNSUPPORTED;
+    }
+    if (precision < 0 || precision > 1) return G2_ERR_ARG;
+    BatchWork *b = new BatchWork();
+    b->n = n;
+    b->mo = mo;
+    b->mi = mi;
+    b->precision = precision;
+    b->st = ops[0]->stream;
+    for (int i = 0; i < n; i++) {
+        if (!ops[i]) { batch_destroy(b); return G2_ERR_ARG; }
+        b->ops.push_back(ops[i]);
+        KrylovWork *k = new KrylovWork();
+        b->k.push_back(k);
+        const int rc = kw_alloc(k, ops[i]->nvec(), mo, mi, precision);
+        if (rc) { batch_destroy(b); return rc; }
+    }
+    for (int i = 0; i < n;) {
+        BatchGroup g;
+        g.op = ops[i];
+        g.first = i;
+        g.n = (i + 1 < n && ops[i + 1] == ops[i]) ? 2 : 1;
+        b->groups.push_back(g);
+        i += g.n;
+    }
+    if (cudaMalloc(&b->d_active, sizeof(int) * n) != cudaSuccess) { batch_destroy(b); return G2_ERR_NOMEM; }
+    b->h_active.assign(n, 1);
+    b->dev_active.assign(n, -1);
+    b->inner_graph_applies.assign(n, 0);
+    b->history.resize(n);
+    *out = b;
+    return G2_OK;
+}
+
+void batch_free(void *h) { batch_destroy(reinterpret_cast<BatchWork *>(h)); }
+
+int batch_history(void *h, int i, double *out, int max_len)
+{
+    BatchWork *b = reinterpret_cast<BatchWork *>(h);
+    if (!b || i < 0 || i >= b->n) return 0;
+    const int m = (int)b->history[i].size() < max_len ? (int)b->history[i].size() : max_len;
+    for (int j = 0; j < m; j++) out[j] = b->history[i][j];
+    return m;
+}
+
+// applies of the inner level: in_i -> out_i for every instance, paired where two instances share an
+// operator (complex64); flag selects the gate of the single applies (F_SOLVER or F_KRYLOV)
+template <typename CI, typename FIn, typename FOut>
+static int batch_apply(BatchWork *b, FIn in, FOut out, int flag, cudaStream_t st)
+{
+    for (const BatchGroup &g : b->groups) {
+        if (g.n == 2 && sizeof(CI) == sizeof(float2)) {
+            float2 *U1 = nullptr, *Uh = nullptr;
+            int rc = ie_pair_scratch(g.op, &U1, &Uh);
+            if (rc) return rc;
+            rc = ie_apply_pair32(g.op, reinterpret_cast<const float2 *>(in(g.first)),
+                                 reinterpret_cast<const float2 *>(in(g.first + 1)),
+                                 reinterpret_cast<float2 *>(out(g.first)), reinterpret_cast<float2 *>(out(g.first + 1)),
+                                 st, U1, Uh);
+            if (rc == G2_OK) {
+                b->k[g.first]->applies32++;
+                b->k[g.first + 1]->applies32++;
+                continue;
+            }
+            if (rc != G2_ERR_UNSUPPORTED) return rc;
+        }
+        for (int i = g.first; i < g.first + g.n; i++) {
+            const int rc = apply_prec<CI>(g.op, in(i), out(i), st, b->k[i]->Li.flags + flag);
+            if (rc) return rc;
+            if (sizeof(CI) == sizeof(float2)) b->k[i]->applies32++;
+            else b->k[i]->applies64++;
+        }
+    }
+    return G2_OK;
+}
+
+// one inner GMRES cycle (x0 = b = v) for every instance: the lockstep form of inner_solve
+template <typename CI>
+static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
+{
+    const int n = b->n;
+    for (int i = 0; i < n; i++) {
+        KrylovWork *k = b->k[i];
+        Level &L = k->Li;
+        const int g = vec_grid(k->N);
+        k_zero_level<<<1, 256, 0, st>>>(L); g2_count_launches(1);
+        norm2<CI>(k, reinterpret_cast<const CI *>(k->vin), L.scal + S_NRM2, b->d_active + i, st);
+        k_set_bn_masked<<<1, 1, 0, st>>>(L, b->d_active + i); g2_count_launches(1);
+        k_copy_or_zero<CI><<<g, kVT, 0, st>>>(reinterpret_cast<CI *>(k->xin), reinterpret_cast<const CI *>(k->vin),
+                                             L.scal, k->N); g2_count_launches(1);
+    }
+    auto vin = [&](int i) { return reinterpret_cast<const CI *>(b->k[i]->vin); };
+    auto ri = [&](int i) { return reinterpret_cast<CI *>(b->k[i]->ri); };
+    int rc = batch_apply<CI>(b, vin, ri, F_SOLVER, st);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++) {
+        KrylovWork *k = b->k[i];
+        Level &L = k->Li;
+        const int g = vec_grid(k->N);
+        const int *solver = L.flags + F_SOLVER;
+        CI *r = reinterpret_cast<CI *>(k->ri);
+        k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(r, 1.0, reinterpret_cast<const CI *>(k->vin), -1.0, r, k->N, solver); g2_count_launches(1);
+        norm2<CI>(k, r, L.scal + S_NRM2, solver, st);
+        k_set_beta<<<1, 1, 0, st>>>(L, tol); g2_count_launches(1);
+        k_cycle_start<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
+        k_scale_by<CI><<<g, kVT, 0, st>>>(reinterpret_cast<CI *>(k->Vi), r, L.scal, S_BETA, k->N, solver); g2_count_launches(1);
+    }
+    for (int j = 0; j < b->mi; j++) {
+        auto vj = [&](int i) { return reinterpret_cast<const CI *>(b->k[i]->Vi) + (size_t)j * b->k[i]->N; };
+        auto wi = [&](int i) { return reinterpret_cast<CI *>(b->k[i]->wi); };
+        if ((rc = batch_apply<CI>(b, vj, wi, F_KRYLOV, st))) return rc;
+        for (int i = 0; i < n; i++) {
+            KrylovWork *k = b->k[i];
+            Level &L = k->Li;
+            const int g = vec_grid(k->N);
+            const int *krylov = L.flags + F_KRYLOV;
+            CI *Vi = reinterpret_cast<CI *>(k->Vi);
+            cgs<CI>(k, L, Vi, j, reinterpret_cast<CI *>(k->wi), krylov, st);
+            k_scale_by<CI><<<g, kVT, 0, st>>>(Vi + (size_t)(j + 1) * k->N, reinterpret_cast<const CI *>(k->wi), L.scal,
+                                              S_DNORMW, k->N, krylov); g2_count_launches(1);
+            k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, krylov); g2_count_launches(1);
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        KrylovWork *k = b->k[i];
+        Level &L = k->Li;
+        const int g = vec_grid(k->N);
+        const int *solver = L.flags + F_SOLVER;
+        CI *x = reinterpret_cast<CI *>(k->xin);
+        k_trisolve<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
+        k_lincomb<CI, CI><<<g, kVT, 0, st>>>(x, 1.0, x, reinterpret_cast<const CI *>(k->Vi), k->N, L.y, L.flags + F_L,
+                                             k->N, solver); g2_count_launches(1);
+    }
+    return G2_OK;
+}
+
+// the inner cycle of all instances: eager on first use, then one captured graph replayed
+template <typename CI>
+static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
+{
+    if (b->h_active != b->dev_active) {
+        G2_CUDA_CHECK(cudaMemcpyAsync(b->d_active, b->h_active.data(), sizeof(int) * b->n, cudaMemcpyHostToDevice, st));
+        b->dev_active = b->h_active;
+    }
+    std::vector<int> cv;
+    for (IeOp *op : b->ops) { cv.push_back(op->contract_variant[0]); cv.push_back(op->contract_variant[1]); }
+    const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
+    const bool graphs = !(ng && ng[0] == '1');
+    if (b->inner_exec && (b->inner_tol != tol || b->cv != cv)) {
+        cudaGraphExecDestroy(b->inner_exec);
+        b->inner_exec = nullptr;
+        b->inner_uses = 0;
+    }
+    auto credit = [&]() {
+        g2_count_launches(b->inner_graph_launches);
+        for (int i = 0; i < b->n; i++) {
+            if (sizeof(CI) == sizeof(float2)) b->k[i]->applies32 += b->inner_graph_applies[i];
+            else b->k[i]->applies64 += b->inner_graph_applies[i];
+        }
+    };
+    if (b->inner_exec) {
+        G2_CUDA_CHECK(cudaGraphLaunch(b->inner_exec, st));
+        credit();
+        return G2_OK;
+    }
+    if (!graphs || b->inner_uses++ == 0) return batch_inner<CI>(b, tol, st);
+    std::vector<int> a0(b->n);
+    for (int i = 0; i < b->n; i++) a0[i] = b->k[i]->applies32 + b->k[i]->applies64;
+    const long long l0 = g2_launch_total();
+    cudaGraph_t graph = nullptr;
+    G2_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = batch_inner<CI>(b, tol, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (rc) return rc;
+    if (ce != cudaSuccess) {
+        g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
+        return G2_ERR_CUDA;
+    }
+    b->inner_graph_launches = (int)(g2_launch_total() - l0);
+    for (int i = 0; i < b->n; i++) {
+        KrylovWork *k = b->k[i];
+        b->inner_graph_applies[i] = k->applies32 + k->applies64 - a0[i];
+        if (sizeof(CI) == sizeof(float2)) k->applies32 -= b->inner_graph_applies[i];
+        else k->applies64 -= b->inner_graph_applies[i];
+    }
+    ce = cudaGraphInstantiate(&b->inner_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+        g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
+        b->inner_exec = nullptr;
+        return G2_ERR_CUDA;
+    }
+    b->inner_tol = tol;
+    b->cv = cv;
+    G2_CUDA_CHECK(cudaGraphLaunch(b->inner_exec, st));
+    credit();
+    return G2_OK;
+}
+
+// per-instance host copies of the outer level's scalars and flags, one synchronisation for all
+struct BatchScal {
+    double s[S_NSCAL];
+    int f[F_NFLAGS];
+};
+static int batch_pull(BatchWork *b, std::vector<BatchScal> &h, cudaStream_t st)
+{
+    for (int i = 0; i < b->n; i++) {
+        if (!b->h_active[i]) continue;
+        G2_CUDA_CHECK(cudaMemcpyAsync(h[i].s, b->k[i]->Lo.scal, sizeof(h[i].s), cudaMemcpyDeviceToHost, st));
+        G2_CUDA_CHECK(cudaMemcpyAsync(h[i].f, b->k[i]->Lo.flags, sizeof(h[i].f), cudaMemcpyDeviceToHost, st));
+    }
+    G2_CUDA_CHECK(cudaStreamSynchronize(st));
+    for (IeOp *op : b->ops) {
+        const int rc = ie_check_device_error(op);
+        if (rc) return rc;
+    }
+    return G2_OK;
+}
+
+// FinalActions of instance i (gmres.F90:382-421) after the host learned that it stops
+template <typename CI>
+static void batch_final_launch(BatchWork *b, int i, cudaStream_t st, int &rc)
+{
+    KrylovWork *k = b->k[i];
+    Level &L = k->Lo;
+    const int g = vec_grid(k->N);
+    CI *Z = reinterpret_cast<CI *>(k->Zo);
+    k_trisolve<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+    k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, k->N, L.y, L.flags + F_L, k->N, nullptr); g2_count_launches(1);
+    if ((rc = ie_apply_device64(b->ops[i], k->x, k->r0, st))) return;
+    k->applies64++;
+    k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, k->N, nullptr); g2_count_launches(1);
+    norm2<double2>(k, k->r0, L.scal + S_NRM2, nullptr, st);
+}
+
+template <typename CI>
+static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT *info, cudaStream_t st)
+{
+    const int n = b->n, M = b->mo;
+    const double tol = ctl.misfit;
+    std::vector<BatchScal> h(n);
+    std::vector<double> bn(n, 0.0), bea(n, -1.0);
+    std::vector<int> iter(n, 0), converged(n, 0), finishing(n, 0);
+    int rc = G2_OK;
+    char msg[256];
+    for (int i = 0; i < n; i++) {
+        b->history[i].clear();
+        b->h_active[i] = 1;
+        info[i].iterations = 0;
+        info[i].bea = -1.0;
+        info[i].be = -1.0;
+        info[i].stat = -1;
+    }
+    // gmres.F90:129-168 for every instance
+    for (int i = 0; i < n; i++) {
+        KrylovWork *k = b->k[i];
+        k_zero_level<<<1, 256, 0, st>>>(k->Lo); g2_count_launches(1);
+        norm2<double2>(k, k->b, k->Lo.scal + S_NRM2, nullptr, st);
+        k_set_bn<<<1, 1, 0, st>>>(k->Lo); g2_count_launches(1);
+    }
+    if ((rc = batch_pull(b, h, st))) return rc;
+    for (int i = 0; i < n; i++) {
+        KrylovWork *k = b->k[i];
+        bn[i] = h[i].s[S_BN];
+        if (bn[i] < ZERO_THRESHOLD) {
+            cudaMemsetAsync(k->x, 0, sizeof(double2) * k->N, st);
+            info[i].stat = 1;
+            b->h_active[i] = 0;
+            continue;
+        }
+        const int g = vec_grid(k->N);
+        if ((rc = ie_apply_device64(b->ops[i], k->x, k->r0, st))) return rc;
+        k->applies64++;
+        k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, k->N, nullptr); g2_count_launches(1);
+        k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->w, 1.0, k->r0, 0.0, (const double2 *)nullptr, k->N, nullptr); g2_count_launches(1);
+        norm2<double2>(k, k->w, k->Lo.scal + S_NRM2, nullptr, st);
+        k_set_beta<<<1, 1, 0, st>>>(k->Lo, tol); g2_count_launches(1);
+    }
+    if ((rc = batch_pull(b, h, st))) return rc;
+    for (int i = 0; i < n; i++) {
+        if (!b->h_active[i]) continue;
+        if (h[i].s[S_BETA] / bn[i] < tol) {
+            info[i].stat = 1;
+            info[i].be = h[i].s[S_BETA] / bn[i];
+            b->h_active[i] = 0;
+        }
+    }
+    auto any_active = [&]() {
+        for (int i = 0; i < n; i++)
+            if (b->h_active[i]) return true;
+        return false;
+    };
+    while (any_active()) {
+        for (int i = 0; i < n; i++) {
+            if (!b->h_active[i]) continue;
+            KrylovWork *k = b->k[i];
+            k_cycle_start<<<1, 1, 0, st>>>(k->Lo, nullptr); g2_count_launches(1);
+            k_scale_by<double2><<<vec_grid(k->N), kVT, 0, st>>>(k->Vo, k->w, k->Lo.scal, S_BETA, k->N, nullptr); g2_count_launches(1);
+        }
+        bool cycle_done = false;
+        for (int j = 0; j < M && !cycle_done; j++) {
+            for (int i = 0; i < n; i++) {
+                if (!b->h_active[i]) continue;
+                KrylovWork *k = b->k[i];
+                k_axpby<CI, double2, double2><<<vec_grid(k->N), kVT, 0, st>>>(
+                    reinterpret_cast<CI *>(k->vin), 1.0, k->Vo + (size_t)j * k->N, 0.0, (const double2 *)nullptr, k->N,
+                    nullptr); g2_count_launches(1);
+            }
+            if ((rc = batch_inner_fixed<CI>(b, tol, st))) return rc;
+            for (int i = 0; i < n; i++) {
+                if (!b->h_active[i]) continue;
+                KrylovWork *k = b->k[i];
+                const int g = vec_grid(k->N);
+                CI *Zj = reinterpret_cast<CI *>(k->Zo) + (size_t)j * k->N;
+                k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, k->N, nullptr); g2_count_launches(1);
+                if (sizeof(CI) == sizeof(double2)) {
+                    if ((rc = ie_apply_device64(b->ops[i], reinterpret_cast<const double2 *>(Zj), k->w, st))) return rc;
+                } else {
+                    k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, k->N, nullptr); g2_count_launches(1);
+                    if ((rc = ie_apply_device64(b->ops[i], k->tmp, k->w, st))) return rc;
+                }
+                k->applies64++;
+                cgs<double2>(k, k->Lo, k->Vo, j, k->w, nullptr, st);
+                k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo + (size_t)(j + 1) * k->N, k->w, k->Lo.scal, S_DNORMW, k->N, nullptr); g2_count_launches(1);
+                k_arnoldi_finish<<<1, 1, 0, st>>>(k->Lo, j, tol, nullptr); g2_count_launches(1);
+            }
+            if ((rc = batch_pull(b, h, st))) return rc;
+            for (int i = 0; i < n; i++) {
+                if (!b->h_active[i]) continue;
+                bea[i] = h[i].s[S_BEA];
+                if (!std::isfinite(bea[i])) {
+                    g2_set_error_msg("FGMRES: non-finite Arnoldi misfit");
+                    return G2_ERR_NUMERIC;
+                }
+                b->history[i].push_back(bea[i]);
+                std::snprintf(msg, sizeof(msg), "FGMRES outer  iteration:%5d Arnoldy misfit: %10.3E  (instance %d)",
+                              (int)b->history[i].size(), bea[i], i);
+                g2_log(msg);
+                if (bea[i] < tol) {
+                    converged[i] = 1;
+                    finishing[i] = 1;
+                    b->h_active[i] = 0;
+                }
+            }
+            if (!any_active()) cycle_done = true;
+        }
+        // end of the cycle for the instances still running: restart or give up (gmres.F90:186-212)
+        for (int i = 0; i < n; i++) {
+            if (!b->h_active[i]) continue;
+            KrylovWork *k = b->k[i];
+            const int g = vec_grid(k->N);
+            iter[i]++;
+            if (iter[i] >= ctl.fgmres_maxit) {
+                finishing[i] = 1;
+                b->h_active[i] = 0;
+                continue;
+            }
+            k_trisolve<<<1, 1, 0, st>>>(k->Lo, nullptr); g2_count_launches(1);
+            k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, reinterpret_cast<const CI *>(k->Zo), k->N,
+                                                      k->Lo.y, k->Lo.flags + F_L, k->N, nullptr); g2_count_launches(1);
+            k_restart_g<<<1, 1, 0, st>>>(k->Lo); g2_count_launches(1);
+            k_copy_g<<<1, 64, 0, st>>>(k->Lo); g2_count_launches(1);
+            k_lincomb<double2, double2><<<g, kVT, 0, st>>>(k->w, 0.0, (const double2 *)nullptr, k->Vo, k->N, k->Lo.y,
+                                                           k->Lo.flags + F_L, k->N, nullptr); g2_count_launches(1);
+        }
+        // instances that stopped in this cycle: final actions now (their own kernels only)
+        for (int i = 0; i < n; i++) {
+            if (!finishing[i]) continue;
+            batch_final_launch<CI>(b, i, st, rc);
+            if (rc) return rc;
+        }
+        bool any_fin = false;
+        for (int i = 0; i < n; i++) any_fin = any_fin || finishing[i];
+        if (any_fin) {
+            // read the true residuals of the instances that finished (pull reads active ones only)
+            for (int i = 0; i < n; i++)
+                if (finishing[i])
+                    G2_CUDA_CHECK(cudaMemcpyAsync(h[i].s, b->k[i]->Lo.scal, sizeof(h[i].s), cudaMemcpyDeviceToHost, st));
+            G2_CUDA_CHECK(cudaStreamSynchronize(st));
+            for (int i = 0; i < n; i++) {
+                if (!finishing[i]) continue;
+                const double be = std::sqrt(h[i].s[S_NRM2]) / bn[i];
+                info[i].iterations = (int)b->history[i].size();
+                info[i].bea = bea[i];
+                info[i].be = be;
+                info[i].stat = converged[i] ? (be >= tol ? 2 : 1) : -1;
+                finishing[i] = 0;
+            }
+        }
+    }
+    return G2_OK;
+}
+
+int batch_solve_device(void *h, const double2 *const *d_Ebkg, double2 *const *d_Esol, const double2 *const *d_E0,
+                       const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT *info)
+{
+    BatchWork *b = reinterpret_cast<BatchWork *>(h);
+    if (!b) return G2_ERR_STATE;
+    if (ctl.fgmres_buf != b->mo || ctl.gmres_buf != b->mi || ctl.precision != b->precision) {
+        g2_set_error_msg("batched solve: buffer sizes or precision differ from the batch's");
+        return G2_ERR_ARG;
+    }
+    cudaStream_t st = b->st;
+    for (IeOp *op : b->ops)
+        if (op->stream != st) G2_CUDA_CHECK(cudaStreamSynchronize(op->stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    for (int i = 0; i < b->n; i++) {
+        IeOp *op = b->ops[i];
+        KrylovWork *k = b->k[i];
+        k->applies32 = k->applies64 = 0;
+        const int g = vec_grid(k->N);
+        // SolveEquation (ie_solver_module.F90:62-80): rhs = sqrt(Re sb) E_bkg; guess = E0/a or rhs
+        k_rhs<<<g, 256, 0, st>>>(k->b, d_Ebkg[i], op->d_post64, (size_t)op->Nx * op->Ny, op->Nz); g2_count_launches(1);
+        if (d_E0 && d_E0[i]) {
+            k_scale_asig<<<g, 256, 0, st>>>(k->x, d_E0[i], op->d_asig64, op->cells(), true); g2_count_launches(1);
+        } else {
+            G2_CUDA_CHECK(cudaMemcpyAsync(k->x, k->b, sizeof(double2) * k->N, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    int rc = b->precision == 0 ? batch_outer<double2>(b, ctl, info, st) : batch_outer<float2>(b, ctl, info, st);
+    if (rc) return rc;
+    for (int i = 0; i < b->n; i++) {
+        IeOp *op = b->ops[i];
+        KrylovWork *k = b->k[i];
+        k_scale_asig<<<vec_grid(k->N), 256, 0, st>>>(d_Esol[i], k->x, op->d_asig64, op->cells(), false); g2_count_launches(1);
+    }
+    cudaEventRecord(e1, st);
+    G2_CUDA_CHECK(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int i = 0; i < b->n; i++) {
+        info[i].applies_fp64 = b->k[i]->applies64;
+        info[i].applies_fp32 = b->k[i]->applies32;
+        info[i].device_ms = ms;
+        b->ops[i]->mult_num += b->k[i]->applies64 + b->k[i]->applies32;
+    }
+    for (IeOp *op : b->ops) {
+        const int e = ie_check_device_error(op);
+        if (e) return e;
+    }
+    return G2_OK;
+}
+
+int batch_stage(void *h, double2 **d_stage, size_t *N)
+{
+    BatchWork *b = reinterpret_cast<BatchWork *>(h);
+    if (!b) return G2_ERR_STATE;
+    size_t nmax = 0;
+    for (IeOp *op : b->ops) nmax = op->nvec() > nmax ? op->nvec() : nmax;
+    if (!b->d_stage) G2_CUDA_CHECK(cudaMalloc(&b->d_stage, sizeof(double2) * nmax * 3 * b->n));
+    *d_stage = b->d_stage;
+    *N = nmax;
+    return G2_OK;
+}
+
+int batch_size(void *h) { return h ? reinterpret_cast<BatchWork *>(h)->n : 0; }
+IeOp *batch_op(void *h, int i) { return reinterpret_cast<BatchWork *>(h)->ops[i]; }

@@ -148,6 +148,29 @@ int giem2g_solve_device(void *ie, const void *d_E_bkg, void *d_Esol, const void 
 /* Outer Arnoldi misfit after each outer iteration of the last solve; returns the count copied. */
 int giem2g_get_misfit_history(void *ie, double *out, int max_len);
 
+/* ---- batched solves -----------------------------------------------------------
+ * The reference solves one (frequency, polarisation) after another (giem2g.F90:336-373).  A batch
+ * holds n instances, each an operator handle (one per frequency, already through
+ * giem2g_calc_fft_of_ie_kernel and giem2g_set_anomaly_conductivity); the same handle may appear
+ * twice in a row for the two polarisations of one frequency.  A batched solve runs every instance's
+ * nested FGMRES in lockstep on ies[0]'s stream: one captured inner cycle serves all instances, and
+ * in mixed precision consecutive instances of one operator share every tensor read.  Each instance
+ * keeps its own iterates, misfit history and status; converged instances are masked off.  The
+ * buffer sizes and precision of ctl are fixed at creation.  Returns NULL on error. */
+void *giem2g_batch_create(void *const *ies, int n, GIEM2G_FGMRES_CTL ctl);
+/* device vectors: d_E_bkg[i], d_Esol[i] complex128 of instance i's size; d_E0 (or d_E0[i]) may be NULL */
+int giem2g_batch_solve_device(void *batch, const void *const *d_E_bkg, void *const *d_Esol,
+                              const void *const *d_E0, GIEM2G_FGMRES_CTL ctl, GIEM2G_RESULT *info);
+/* the same with host arrays (copied in and out every call) */
+int giem2g_solve_batched(void *batch, const void *const *E_bkg, void *const *Esol, const void *const *E0,
+                         GIEM2G_FGMRES_CTL ctl, GIEM2G_RESULT *info);
+int giem2g_batch_misfit_history(void *batch, int i, double *out, int max_len);
+void giem2g_batch_delete(void *batch);
+/* nv device vectors through one operator; precision 1 applies them two at a time with shared tensor
+ * reads, precision 0 one at a time. */
+int giem2g_apply_ie_operator_device_batch(void *ie, int nv, const void *const *d_in, void *const *d_out,
+                                          int precision);
+
 #ifdef __cplusplus
 }
 #endif

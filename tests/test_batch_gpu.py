@@ -1,0 +1,139 @@
+"""Batched applies and batched (lockstep) solves against the single-instance path and the oracle.
+
+Tolerances: complex64 applies 2e-5 relative to the oracle (as the single apply); FP64 batched solves
+reproduce the single solves (same iteration counts and status, solutions within 1e-12); mixed batched
+solves keep the single solves' status and reach the FP64 solution within 1e-5.
+"""
+import numpy as np
+import pytest
+
+from giem2g_b200.sources import plane_wave_integral
+from giem2g_b200.synthetic import config_small_block, csiga_from_sigma
+from tests.helpers import random_sigma, random_spatial_tensor, random_vec, rel, tiny_model
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 2e-5
+
+
+def _op_random(g2, m, seed=3):
+    symm, asym = random_spatial_tensor(m, seed=seed)
+    op = g2.IEOperator.from_model(m)
+    op.set_background(m.csigma, m.thick, m.omega)
+    op.set_ie_kernel_spatial(symm, asym)
+    op.calc_fft_of_ie_kernel()
+    sig = random_sigma(m, seed)
+    op.set_anomaly_conductivity(csiga_from_sigma(sig, m.freq))
+    return op, symm, asym, sig
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (4, 8, 16), (4, 4, 32), (2, 4, 48), (8, 4, 5)])
+def test_pair_apply_matches_oracle(g2lib, orc, shape):
+    import torch
+    m = tiny_model(*shape)
+    op, symm, asym, sig = _op_random(g2lib, m)
+    csigb, sqsigb = orc.background_cells(m)
+    sh, ah = orc.tensor_spectrum(m.Nx, m.Ny, m.Nz, symm, asym)
+    csiga = csiga_from_sigma(sig, m.freq)
+    vs = [random_vec(m, s) for s in (21, 22, 23)]
+    d_in = [torch.from_numpy(v.ravel()).to("cuda", torch.complex64) for v in vs]
+    d_out = [torch.empty_like(x) for x in d_in]
+    g2lib.apply_device_batch(op, [x.data_ptr() for x in d_in], [y.data_ptr() for y in d_out], 1)
+    single = torch.empty_like(d_in[0])
+    for v, x, y in zip(vs, d_in, d_out):
+        ref = orc.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v)
+        got = y.cpu().numpy().astype(np.complex128).reshape(ref.shape)
+        assert rel(got, ref) < TOL32
+        op.apply_device(x.data_ptr(), single.data_ptr(), 1)
+        torch.cuda.synchronize()
+        assert rel(got, single.cpu().numpy().astype(np.complex128).reshape(ref.shape)) < TOL32
+    op.check_device_error()
+    op.delete()
+
+
+def test_batch_apply_fp64_equals_single(g2lib):
+    import torch
+    m = tiny_model(8, 8, 6)
+    op, *_ = _op_random(g2lib, m)
+    d_in = [torch.from_numpy(random_vec(m, s).ravel()).to("cuda") for s in (1, 2, 3)]
+    d_out = [torch.empty_like(x) for x in d_in]
+    g2lib.apply_device_batch(op, [x.data_ptr() for x in d_in], [y.data_ptr() for y in d_out], 0)
+    for x, y in zip(d_in, d_out):
+        ref = torch.empty_like(x)
+        op.apply_device(x.data_ptr(), ref.data_ptr(), 0)
+        torch.cuda.synchronize()
+        assert torch.equal(y, ref)
+    op.delete()
+
+
+def _two_frequency_setup(g2):
+    m1, sig = config_small_block()
+    m2 = m1.with_freq(10.0)
+    ops = []
+    for m in (m1, m2):
+        op = g2.IEOperator.from_model(m)
+        op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+        op.calc_fft_of_ie_kernel()
+        op.set_anomaly_sigma(sig, m.freq)
+        ops.append(op)
+    # instances: (1 Hz, EY), (1 Hz, EX), (10 Hz, EY)
+    inst = [(ops[0], plane_wave_integral(m1, 1)), (ops[0], plane_wave_integral(m1, 0)),
+            (ops[1], plane_wave_integral(m2, 1))]
+    return ops, inst
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-8), (1, 1e-6)])
+def test_batched_solve_matches_single(g2lib, precision, tol):
+    import torch
+    ops, inst = _two_frequency_setup(g2lib)
+    d_e = [torch.from_numpy(np.ascontiguousarray(e).ravel()).to("cuda") for _, e in inst]
+    d_s = [torch.empty_like(x) for x in d_e]
+    single, infos1 = [], []
+    for (op, _), x in zip(inst, d_e):
+        y = torch.empty_like(x)
+        infos1.append(op.solve_device(x.data_ptr(), y.data_ptr(), None, tol=tol, precision=precision))
+        single.append(y)
+    ref64 = []
+    for (op, _), x in zip(inst, d_e):
+        y = torch.empty_like(x)
+        op.solve_device(x.data_ptr(), y.data_ptr(), None, tol=1e-10, precision=0)
+        ref64.append(y)
+    b = g2lib.Batch([op for op, _ in inst], precision=precision)
+    infos = b.solve_device([x.data_ptr() for x in d_e], [y.data_ptr() for y in d_s], tol=tol)
+    torch.cuda.synchronize()
+    for i in range(len(inst)):
+        assert infos[i].stat == infos1[i].stat == 1
+        assert len(infos[i].misfits) == infos[i].iterations
+        if precision == 0:
+            assert infos[i].iterations == infos1[i].iterations
+            assert rel(d_s[i].cpu().numpy(), single[i].cpu().numpy()) < 1e-12
+            assert np.allclose(infos[i].misfits, infos1[i].misfits, rtol=1e-10, atol=0)
+        else:
+            assert abs(infos[i].iterations - infos1[i].iterations) <= 1
+            assert infos[i].be < tol
+            assert rel(d_s[i].cpu().numpy(), ref64[i].cpu().numpy()) < 1e-5
+    # the host-array entry point gives the device result
+    outs, infos_h = b.solve([e for _, e in inst], tol=tol)
+    for i in range(len(inst)):
+        assert infos_h[i].iterations == infos[i].iterations
+        assert rel(outs[i].ravel(), d_s[i].cpu().numpy()) < 1e-12
+    b.delete()
+    for op in ops:
+        op.delete()
+
+
+def test_batched_solve_zero_rhs_instance(g2lib):
+    import torch
+    ops, inst = _two_frequency_setup(g2lib)
+    d_e = [torch.from_numpy(np.ascontiguousarray(inst[0][1]).ravel()).to("cuda"),
+           torch.zeros(ops[0].nvec, dtype=torch.complex128, device="cuda")]
+    d_s = [torch.full_like(x, 1.0) for x in d_e]
+    b = g2lib.Batch([ops[0], ops[0]], precision=1)
+    infos = b.solve_device([x.data_ptr() for x in d_e], [y.data_ptr() for y in d_s], tol=1e-6)
+    torch.cuda.synchronize()
+    assert infos[0].stat == 1 and infos[0].iterations > 0
+    assert infos[1].stat == 1 and infos[1].iterations == 0
+    assert float(d_s[1].abs().max()) == 0.0
+    b.delete()
+    for op in ops:
+        op.delete()
