@@ -40,6 +40,7 @@ struct Level {
     double2 *hpass = nullptr, *hnext = nullptr, *y = nullptr;
     double *scal = nullptr;
     int *flags = nullptr;
+    unsigned *counter = nullptr;  // blocks done, for the last-block reductions (back to 0 after each use)
 };
 
 G2_HD int hix(int i, int j, int m) { return i + j * (m + 1); }
@@ -87,109 +88,19 @@ G2_D void block_reduce_store_r(R (&ax)[KM + 1], R (&ay)[KM + 1], double2 *part)
     }
 }
 
-// dots: part[b][k] = sum_i conj(V_k[i]) w[i], k < K; part[b][KMAX] = sum |w|^2
-template <typename C, int K>
-__global__ void __launch_bounds__(kVT) k_dots_t(const C *__restrict__ V, size_t ld, const C *__restrict__ w,
-                                                size_t N, double2 *part, const int *gate)
-{
-    if (gate && *gate == 0) return;
-    using R = typename RealOf<C>::T;
-    R ax[K + 1], ay[K + 1];
-#pragma unroll
-    for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
-        const C wv = w[i];
-        ax[K] += wv.x * wv.x + wv.y * wv.y;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const C v = V[(size_t)k * ld + i];
-            ax[k] += v.x * wv.x + v.y * wv.y;
-            ay[k] += v.x * wv.y - v.y * wv.x;
-        }
-    }
-    block_reduce_store_r<K, R>(ax, ay, part);
-}
-
-// fused CGS pass: w -= V h; then part[b][k] = sum conj(V_k) w', part[b][KMAX] = ||w'||^2
-// (V is read twice per element; the second read hits L1)
-template <typename C, int K>
-__global__ void __launch_bounds__(kVT) k_cgs_pass_t(const C *__restrict__ V, size_t ld, C *__restrict__ w, size_t N,
-                                                    const double2 *__restrict__ h, double2 *part, const int *gate1,
-                                                    const int *gate2)
-{
-    if ((gate1 && *gate1 == 0) || (gate2 && *gate2 == 0)) return;
-    using R = typename RealOf<C>::T;
-    constexpr int KA = K > 0 ? K : 1;
-    __shared__ double2 hs[KA];
-    if (threadIdx.x < K) hs[threadIdx.x] = h[threadIdx.x];
-    __syncthreads();
-    R ax[K + 1], ay[K + 1];
-#pragma unroll
-    for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
-        C wv = w[i];
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const C v = V[(size_t)k * ld + i];
-            const R hx = (R)hs[k].x, hy = (R)hs[k].y;  // shared-memory broadcast
-            wv.x -= v.x * hx - v.y * hy;
-            wv.y -= v.x * hy + v.y * hx;
-        }
-        w[i] = wv;
-        ax[K] += wv.x * wv.x + wv.y * wv.y;
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            const C v = V[(size_t)k * ld + i];
-            ax[k] += v.x * wv.x + v.y * wv.y;
-            ay[k] += v.x * wv.y - v.y * wv.x;
-        }
-    }
-    block_reduce_store_r<K, R>(ax, ay, part);
-}
-
-// sum the block partials, one CTA per column: out[k] = sum_b part[b][k] (k < K), *nrm2 = sum_b part[b][KMAX]
-__global__ void k_reduce_parts(const double2 *__restrict__ part, int nb, int K, double2 *out, double *nrm2,
-                               const int *gate1, const int *gate2)
-{
-    if ((gate1 && *gate1 == 0) || (gate2 && *gate2 == 0)) return;
-    __shared__ double2 sm[256];
-    const int k = blockIdx.x;
-    const int col = (k == K) ? KMAX : k;
-    double2 s = make_double2(0.0, 0.0);
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        s.x += part[(size_t)b * (KMAX + 1) + col].x;
-        s.y += part[(size_t)b * (KMAX + 1) + col].y;
-    }
-    sm[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) {
-            sm[threadIdx.x].x += sm[threadIdx.x + o].x;
-            sm[threadIdx.x].y += sm[threadIdx.x + o].y;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        if (k < K) out[k] = sm[0];
-        else if (nrm2) *nrm2 = sm[0].x;
-    }
-}
-
 // ---- scalar control kernels (one thread) -------------------------------------------------------
 // first CGS pass of step j: H(0..j, j) = h, hpass = h, pass active
-__global__ void k_cgs_first(Level L, int j, const int *gate)
+G2_D void cgs_first_body(Level &L, int j, const double2 *h)
 {
-    if (gate && *gate == 0) return;
     for (int i = 0; i <= j; i++) {
-        L.H[hix(i, j, L.m)] = L.hnext[i];
-        L.hpass[i] = L.hnext[i];
+        L.H[hix(i, j, L.m)] = h[i];
+        L.hpass[i] = h[i];
     }
     L.flags[F_PASS] = 1;
 }
 // after pass p (1-based) subtracted hpass: decide on another pass (gmres.F90:277-280)
-__global__ void k_cgs_next(Level L, int j, int p, const int *gate)
+G2_D void cgs_next_body(Level &L, int j, int p)
 {
-    if ((gate && *gate == 0) || L.flags[F_PASS] == 0) return;
     double dl = 0.0;
     for (int i = 0; i <= j; i++) dl += L.hpass[i].x * L.hpass[i].x + L.hpass[i].y * L.hpass[i].y;
     const double dloo = sqrt(dl), dnormw = sqrt(L.scal[S_NRM2]);
@@ -237,9 +148,8 @@ G2_D void zrotg(double2 &ca, double2 cb, double &c, double2 &s)
 }
 
 // end of Arnoldi step j (gmres.F90:283-326): H(j+1,j), rotations, Arnoldi misfit, exit test
-__global__ void k_arnoldi_finish(Level L, int j, double tol, const int *gate)
+G2_D void arnoldi_finish_body(Level &L, int j, double tol)
 {
-    if (gate && *gate == 0) return;
     const int m = L.m;
     const double dnormw = L.scal[S_DNORMW];
     L.H[hix(j + 1, j, m)] = make_double2(dnormw, 0.0);
@@ -254,6 +164,153 @@ __global__ void k_arnoldi_finish(Level L, int j, double tol, const int *gate)
     L.flags[F_ITER] += 1;
     L.flags[F_L] = j + 1;
     if (bea < tol || j + 1 >= m) L.flags[F_KRYLOV] = 0;
+}
+
+// ---- fused reductions: the last block to finish sums every block's partials ----------------------
+// Each block stores its partials, then counts itself done; the block that counts last reduces all
+// partials in a fixed order (lane-strided sums, shuffle tree: the result does not depend on which block
+// is last) and runs the scalar step that used to be a separate one-thread launch.  It resets the counter
+// for the next use.  Blocks test their gates before any of them can reach the last block, so a flag the
+// last block changes cannot be seen half-way through the grid.
+G2_D bool last_block(unsigned *counter)
+{
+    __shared__ bool am_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (am_last && threadIdx.x == 0) *counter = 0u;
+    return am_last;
+}
+// sums of part[b][col] over blocks for columns 0..K-1 into h[], and of column KMAX into *nrm (one block)
+G2_D void reduce_partials(const double2 *part, int nb, int K, double2 *h, double *nrm)
+{
+    __threadfence();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = warp; k <= K; k += nw) {
+        const int col = (k == K) ? KMAX : k;
+        double sx = 0.0, sy = 0.0;
+        for (int b = lane; b < nb; b += 32) {
+            const double2 v = __ldcg(part + (size_t)b * (KMAX + 1) + col);
+            sx += v.x;
+            sy += v.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        if (lane == 0) {
+            if (k < K) h[k] = make_double2(sx, sy);
+            else if (nrm) *nrm = sx;
+        }
+    }
+    __syncthreads();
+}
+
+// first CGS pass of Arnoldi step j = K-1: h = V^H w, then H(0..j, j) = h, hpass = h
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_dots_first_t(const C *__restrict__ V, size_t ld, const C *__restrict__ w,
+                                                      size_t N, double2 *part, Level L, const int *gate)
+{
+    if (gate && *gate == 0) return;
+    using R = typename RealOf<C>::T;
+    R ax[K + 1], ay[K + 1];
+#pragma unroll
+    for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
+    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+        const C wv = w[i];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const C v = V[(size_t)k * ld + i];
+            ax[k] += v.x * wv.x + v.y * wv.y;
+            ay[k] += v.x * wv.y - v.y * wv.x;
+        }
+    }
+    block_reduce_store_r<K, R>(ax, ay, part);
+    if (!last_block(L.counter)) return;
+    __shared__ double2 hs[KMAX + 1];
+    reduce_partials(part, gridDim.x, K, hs, nullptr);
+    if (threadIdx.x == 0) cgs_first_body(L, K - 1, hs);
+}
+
+// CGS pass p of step j = K-1: w -= V hpass; dots of the new w; then the pass decision (gmres.F90:277-280)
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_cgs_pass_fused_t(const C *__restrict__ V, size_t ld, C *__restrict__ w,
+                                                          size_t N, double2 *part, Level L, int p, const int *gate)
+{
+    if ((gate && *gate == 0) || L.flags[F_PASS] == 0) return;
+    using R = typename RealOf<C>::T;
+    constexpr int KA = K > 0 ? K : 1;
+    __shared__ double2 hsh[KA];
+    if (threadIdx.x < K) hsh[threadIdx.x] = L.hpass[threadIdx.x];
+    __syncthreads();
+    R ax[K + 1], ay[K + 1];
+#pragma unroll
+    for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
+    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+        C wv = w[i];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const C v = V[(size_t)k * ld + i];
+            const R hx = (R)hsh[k].x, hy = (R)hsh[k].y;
+            wv.x -= v.x * hx - v.y * hy;
+            wv.y -= v.x * hy + v.y * hx;
+        }
+        w[i] = wv;
+        ax[K] += wv.x * wv.x + wv.y * wv.y;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const C v = V[(size_t)k * ld + i];
+            ax[k] += v.x * wv.x + v.y * wv.y;
+            ay[k] += v.x * wv.y - v.y * wv.x;
+        }
+    }
+    block_reduce_store_r<K, R>(ax, ay, part);
+    if (!last_block(L.counter)) return;
+    __shared__ double2 hs[KMAX + 1];
+    __shared__ double nrm;
+    reduce_partials(part, gridDim.x, K, hs, &nrm);
+    if (threadIdx.x < K) L.hnext[threadIdx.x] = hs[threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        L.scal[S_NRM2] = nrm;
+        cgs_next_body(L, K - 1, p);
+    }
+}
+
+// ||w||^2 into *nrm2
+template <typename C>
+__global__ void __launch_bounds__(kVT) k_norm2_fused(const C *__restrict__ w, size_t N, double2 *part, double *nrm2,
+                                                     unsigned *counter, const int *gate)
+{
+    if (gate && *gate == 0) return;
+    using R = typename RealOf<C>::T;
+    R ax[1] = {R(0)}, ay[1] = {R(0)};
+    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+        const C wv = w[i];
+        ax[0] += wv.x * wv.x + wv.y * wv.y;
+    }
+    block_reduce_store_r<0, R>(ax, ay, part);
+    if (!last_block(counter)) return;
+    __shared__ double nrm;
+    reduce_partials(part, gridDim.x, 0, nullptr, &nrm);
+    if (threadIdx.x == 0) *nrm2 = nrm;
+}
+
+// end of Arnoldi step j: V_{j+1} = w / ||w||, then the last block runs the Givens/misfit step
+template <typename C>
+__global__ void __launch_bounds__(kVT) k_scale_finish(C *v, const C *w, size_t N, Level L, int j, double tol,
+                                                      const int *gate)
+{
+    if (gate && *gate == 0) return;
+    const double inv = 1.0 / L.scal[S_DNORMW];
+    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+        const double2 x = ld2(w, i);
+        st2(v, i, make_double2(x.x * inv, x.y * inv));
+    }
+    if (!last_block(L.counter)) return;
+    if (threadIdx.x == 0) arnoldi_finish_body(L, j, tol);
 }
 
 // ConstructCurrentSolution's triangular solve (gmres.F90:441-445): y = H(0:L,0:L)^-1 g
@@ -465,13 +522,15 @@ static int alloc_level(Level &L, int m)
     G2_CUDA_CHECK(cudaMalloc(&L.y, sizeof(double2) * (KMAX + 1)));
     G2_CUDA_CHECK(cudaMalloc(&L.scal, sizeof(double) * S_NSCAL));
     G2_CUDA_CHECK(cudaMalloc(&L.flags, sizeof(int) * F_NFLAGS));
+    G2_CUDA_CHECK(cudaMalloc(&L.counter, sizeof(unsigned)));
+    G2_CUDA_CHECK(cudaMemset(L.counter, 0, sizeof(unsigned)));
     G2_CUDA_CHECK(cudaMemset(L.flags, 0, sizeof(int) * F_NFLAGS));
     G2_CUDA_CHECK(cudaMemset(L.scal, 0, sizeof(double) * S_NSCAL));
     return G2_OK;
 }
 static void free_level(Level &L)
 {
-    void *p[] = {L.H, L.cs, L.sn, L.hpass, L.hnext, L.y, L.scal, L.flags};
+    void *p[] = {L.H, L.cs, L.sn, L.hpass, L.hnext, L.y, L.scal, L.flags, L.counter};
     for (void *q : p)
         if (q) cudaFree(q);
     L = Level();
@@ -534,15 +593,14 @@ static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
 
 // ---- launch helpers ------------------------------------------------------------------------------
 template <typename C, int K>
-static void launch_dots_k(KrylovWork *k, const C *V, const C *w, const int *g, cudaStream_t st)
+static void launch_dots_first_k(KrylovWork *k, const C *V, const C *w, Level &L, const int *g, cudaStream_t st)
 {
-    k_dots_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, k->part, g);
+    k_dots_first_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, k->part, L, g);
 }
 template <typename C, int K>
-static void launch_cgs_k(KrylovWork *k, const C *V, C *w, const double2 *h, const int *g1, const int *g2,
-                         cudaStream_t st)
+static void launch_pass_fused_k(KrylovWork *k, const C *V, C *w, Level &L, int p, const int *g, cudaStream_t st)
 {
-    k_cgs_pass_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, h, k->part, g1, g2);
+    k_cgs_pass_fused_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, k->part, L, p, g);
 }
 #define G2_KCASES(F, ...)                                                                                     \
     switch (K) {                                                                                          \
@@ -566,33 +624,31 @@ static void launch_cgs_k(KrylovWork *k, const C *V, C *w, const double2 *h, cons
     }
 
 template <typename C>
-static void dots(KrylovWork *k, const C *V, int K, const C *w, double2 *out, double *nrm2, const int *g1,
-                 const int *g2, cudaStream_t st)
-{
-    G2_KCASES(launch_dots_k, k, V, w, g1 ? g1 : g2, st)
-    g2_count_launches(1);
-    k_reduce_parts<<<K + 1, 256, 0, st>>>(k->part, k->nparts, K, out, nrm2, g1, g2); g2_count_launches(1);
-}
-template <typename C>
 static void norm2(KrylovWork *k, const C *w, double *nrm2, const int *g, cudaStream_t st)
 {
-    k_dots_t<C, 0><<<k->nparts, kVT, 0, st>>>(w, k->N, w, k->N, k->part, g); g2_count_launches(1);
-    k_reduce_parts<<<1, 256, 0, st>>>(k->part, k->nparts, 0, nullptr, nrm2, g, nullptr); g2_count_launches(1);
+    // kernels on one stream run one after another, so any level's counter serves
+    k_norm2_fused<C><<<k->nparts, kVT, 0, st>>>(w, k->N, k->part, nrm2, k->Lo.counter, g); g2_count_launches(1);
 }
 
-// CGS for Arnoldi step j on level L with basis V (j+1 columns) and vector w
+// CGS for Arnoldi step j on level L with basis V (j+1 columns) and vector w: the first pass's dots and
+// up to N_IGS+1 correction passes, each one launch (passes after the decision to stop exit at once)
 template <typename C>
 static void cgs(KrylovWork *k, Level &L, const C *V, int j, C *w, const int *gate, cudaStream_t st)
 {
     const int K = j + 1;
-    dots<C>(k, V, K, w, L.hnext, nullptr, gate, nullptr, st);
-    k_cgs_first<<<1, 1, 0, st>>>(L, j, gate); g2_count_launches(1);
+    G2_KCASES(launch_dots_first_k, k, V, w, L, gate, st)
+    g2_count_launches(1);
     for (int p = 1; p <= N_IGS + 1; p++) {
-        G2_KCASES(launch_cgs_k, k, V, w, L.hpass, gate, L.flags + F_PASS, st)
+        G2_KCASES(launch_pass_fused_k, k, V, w, L, p, gate, st)
         g2_count_launches(1);
-        k_reduce_parts<<<K + 1, 256, 0, st>>>(k->part, k->nparts, K, L.hnext, L.scal + S_NRM2, gate, L.flags + F_PASS); g2_count_launches(1);
-        k_cgs_next<<<1, 1, 0, st>>>(L, j, p, gate); g2_count_launches(1);
     }
+}
+// end of Arnoldi step j: V_{j+1} = w / ||w|| and the Givens / misfit update, one launch
+template <typename C>
+static void arnoldi_tail(KrylovWork *k, Level &L, C *V, int j, const C *w, double tol, const int *gate, cudaStream_t st)
+{
+    k_scale_finish<C><<<vec_grid(k->N), kVT, 0, st>>>(V + (size_t)(j + 1) * k->N, w, k->N, L, j, tol, gate);
+    g2_count_launches(1);
 }
 
 template <typename C> static int apply_prec(IeOp *op, const C *in, C *out, cudaStream_t st, const int *gate);
@@ -634,8 +690,7 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
         k->applies32 += sizeof(CI) == 8 ? 1 : 0;
         k->applies64 += sizeof(CI) == 16 ? 1 : 0;
         cgs<CI>(k, L, Vi, j, wi, krylov, st);
-        k_scale_by<CI><<<g, kVT, 0, st>>>(Vi + (size_t)(j + 1) * N, wi, L.scal, S_DNORMW, N, krylov); g2_count_launches(1);
-        k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, krylov); g2_count_launches(1);
+        arnoldi_tail<CI>(k, L, Vi, j, wi, tol, krylov, st);
     }
     // FinalActions -> ConstructCurrentSolution (gmres.F90:423-458): x = x0 + V y
     k_trisolve<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
@@ -776,8 +831,7 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
             }
             k->applies64++;
             cgs<double2>(k, L, k->Vo, j, k->w, nullptr, st);
-            k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo + (size_t)(j + 1) * N, k->w, L.scal, S_DNORMW, N, nullptr); g2_count_launches(1);
-            k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, nullptr); g2_count_launches(1);
+            arnoldi_tail<double2>(k, L, k->Vo, j, k->w, tol, nullptr, st);
             if ((rc = pull())) return rc;
             bea = h_scal[S_BEA];
             if (!std::isfinite(bea)) {
@@ -1055,9 +1109,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
             const int *krylov = L.flags + F_KRYLOV;
             CI *Vi = reinterpret_cast<CI *>(k->Vi);
             cgs<CI>(k, L, Vi, j, reinterpret_cast<CI *>(k->wi), krylov, st);
-            k_scale_by<CI><<<g, kVT, 0, st>>>(Vi + (size_t)(j + 1) * k->N, reinterpret_cast<const CI *>(k->wi), L.scal,
-                                              S_DNORMW, k->N, krylov); g2_count_launches(1);
-            k_arnoldi_finish<<<1, 1, 0, st>>>(L, j, tol, krylov); g2_count_launches(1);
+            arnoldi_tail<CI>(k, L, Vi, j, reinterpret_cast<const CI *>(k->wi), tol, krylov, st);
         }
     }
     for (int i = 0; i < n; i++) {
@@ -1082,7 +1134,8 @@ static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
         b->dev_active = b->h_active;
     }
     std::vector<int> cv;
-    for (IeOp *op : b->ops) { cv.push_back(op->contract_variant[0]); cv.push_back(op->contract_variant[1]); }
+    for (IeOp *op : b->ops)
+        for (int q = 0; q < 3; q++) cv.push_back(op->contract_variant[q]);
     const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
     const bool graphs = !(ng && ng[0] == '1');
     if (b->inner_exec && (b->inner_tol != tol || b->cv != cv)) {
@@ -1260,8 +1313,7 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
                 }
                 k->applies64++;
                 cgs<double2>(k, k->Lo, k->Vo, j, k->w, nullptr, st);
-                k_scale_by<double2><<<g, kVT, 0, st>>>(k->Vo + (size_t)(j + 1) * k->N, k->w, k->Lo.scal, S_DNORMW, k->N, nullptr); g2_count_launches(1);
-                k_arnoldi_finish<<<1, 1, 0, st>>>(k->Lo, j, tol, nullptr); g2_count_launches(1);
+                arnoldi_tail<double2>(k, k->Lo, k->Vo, j, k->w, tol, nullptr, st);
             }
             if ((rc = batch_pull(b, h, st))) return rc;
             for (int i = 0; i < n; i++) {
