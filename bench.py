@@ -259,7 +259,9 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.synchronize()
     fp64_pair_ms = ev0.elapsed_time(ev1)
 
-    # mixed precision, one polarisation after the other (the reference's order)
+    # mixed precision, one polarisation after the other (the reference's order); one untimed pair first
+    # (work-space reallocation for the precision change, graph capture)
+    solve_pair(1)
     torch.cuda.synchronize()
     ev0.record(stream)
     iy_s, ix_s = solve_pair(1)
@@ -336,8 +338,27 @@ def run_b200(args, rank, world, local_rank):
 
     ms64 = time_apply(0)
     ms32 = time_apply(1)
+
+    def time_pair(reps=20):
+        xs = [torch.randn(n, dtype=torch.complex64, device=dev) for _ in range(2)]
+        ys = [torch.empty_like(x) for x in xs]
+        pi, po = [x.data_ptr() for x in xs], [y.data_ptr() for y in ys]
+        for _ in range(3):
+            g2.apply_device_batch(op, pi, po, 1)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(reps):
+            g2.apply_device_batch(op, pi, po, 1)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        return a0.elapsed_time(a1) / reps
+
+    ms32_pair = time_pair()
     B64 = _algorithmic_bytes(m.Nx, m.Ny, m.Nz, 16)
     B32 = _algorithmic_bytes(m.Nx, m.Ny, m.Nz, 8)
+    # two vectors sharing one tensor read: S*[T + 2*(2*N_vec + NxNy*Nz)]
+    B32P = 2 * B32 - 8 * m.Nx * m.Ny * (2 * m.Nz * (m.Nz + 1) + 2 * m.Nz * m.Nz)
     peaks = _peaks()
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
@@ -378,6 +399,8 @@ def run_b200(args, rank, world, local_rank):
                          "traffic": _profiles_traffic(), "kernel": "FP64 IE apply (5 kernels; contraction dominant)",
                          "bytes_per_launch": B64, "ms_per_launch": ms64, "peak_source": peak_src},
             "apply_c64": {"ms": ms32, "achieved_gbs": ach32, "frac": ach32 / peak, "bytes": B32},
+            "apply_c64_pair": {"ms": ms32_pair, "bytes": B32P, "achieved_gbs": B32P / (ms32_pair * 1e-3) / 1e9,
+                               "frac": B32P / (ms32_pair * 1e-3) / 1e9 / peak},
             "solve": {"mixed_batched_pair_ms": t_max / args.steps * 1e3, "mixed_sequential_pair_ms": mixed_seq_pair_ms,
                       "fp64_pair_ms": fp64_pair_ms,
                       "speedup_vs_fp64_gpu": fp64_pair_ms / (t_max / args.steps * 1e3),

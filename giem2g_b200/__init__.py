@@ -71,7 +71,8 @@ EXPORTED_SYMBOLS = [
     "giem2g_contract_variants", "giem2g_set_contract_variant", "giem2g_kernel_launch_count",
     "giem2g_apply_ie_operator_device_static", "giem2g_batch_create", "giem2g_batch_solve_device",
     "giem2g_solve_batched", "giem2g_batch_misfit_history", "giem2g_batch_delete",
-    "giem2g_apply_ie_operator_device_batch",
+    "giem2g_apply_ie_operator_device_batch", "giem2g_gemm_bf16_tn", "giem2g_im2col3d_bf16",
+    "giem2g_col2im3d_f32",
 ]
 
 
@@ -133,6 +134,9 @@ def lib():
     L.giem2g_batch_delete.argtypes = [vp]
     L.giem2g_batch_delete.restype = None
     L.giem2g_apply_ie_operator_device_batch.argtypes = [vp, ip, pp, pp, ip]
+    L.giem2g_gemm_bf16_tn.argtypes = [vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, vp, vp]
+    L.giem2g_im2col3d_bf16.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
+    L.giem2g_col2im3d_f32.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
     _lib = L
     return L
 
@@ -400,3 +404,17 @@ def apply_device_batch(op, d_in, d_out, precision=1):
     """giem2g_apply_ie_operator_device_batch over lists of device pointers."""
     _check(lib().giem2g_apply_ie_operator_device_batch(op.handle, len(d_in), _ptrs(d_in), _ptrs(d_out), precision),
            "apply_device_batch")
+
+
+def gemm_bf16_tn(A, B, C=None, accumulate=False, err=None, stream=None):
+    """C = A @ B.T on the tcgen05 tensor cores (A [M,K], B [N,K] bf16 CUDA tensors, C [M,N] float32)."""
+    import torch
+    M, K = A.shape
+    N = B.shape[0]
+    if C is None:
+        C = torch.empty(M, N, dtype=torch.float32, device=A.device)
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(lib().giem2g_gemm_bf16_tn(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K, A.stride(0), B.stride(0),
+                                     C.stride(0), 1 if accumulate else 0,
+                                     err.data_ptr() if err is not None else None, s), "gemm_bf16_tn")
+    return C

@@ -377,8 +377,8 @@ void giem2g_apply_ie_operator(void *ie, void *in, void *out)
 int giem2g_set_contract_variant(void *ie, int precision, int variant)
 {
     IeOp *op = resolve(ie);
-    if (!op || precision < 0 || precision > 1) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: bad arguments");
-    const int n = ie_contract_variants(precision, op->Nz);
+    if (!op || precision < 0 || precision > 2) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: bad arguments");
+    const int n = precision == 2 ? ie_contract_pair_variants(op->Nz) : ie_contract_variants(precision, op->Nz);
     if (variant < 0 || (variant > 0 && variant >= n)) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: variant %d of %d", variant, n);
     op->contract_variant[precision] = variant;
     return set_status(0);
@@ -387,7 +387,8 @@ int giem2g_set_contract_variant(void *ie, int precision, int variant)
 int giem2g_contract_variants(void *ie, int precision)
 {
     IeOp *op = resolve(ie);
-    return op ? ie_contract_variants(precision, op->Nz) : 0;
+    if (!op) return 0;
+    return precision == 2 ? ie_contract_pair_variants(op->Nz) : ie_contract_variants(precision, op->Nz);
 }
 
 int giem2g_check_device_error(void *ie)
@@ -543,6 +544,36 @@ int giem2g_apply_ie_operator_device_batch(void *ie, int nv, const void *const *d
         op->mult_num++;
     }
     cudaEventRecord(op->ev1, op->stream);
+    return set_status(0);
+}
+
+int giem2g_gemm_bf16_tn(const void *A, const void *B, float *C, int M, int N, int K, int lda, int ldb, int ldc,
+                        int accumulate, int *d_err, void *stream)
+{
+    static int *own_err = nullptr;
+    if (!d_err) {
+        if (!own_err && (cudaMalloc(&own_err, sizeof(int)) != cudaSuccess || cudaMemset(own_err, 0, sizeof(int)) != cudaSuccess))
+            return fail(G2_ERR_NOMEM, "giem2g_gemm_bf16_tn: error word");
+        d_err = own_err;
+    }
+    const int rc = ie_gemm_bf16_tn(A, B, C, M, N, K, lda, ldb, ldc, accumulate, d_err,
+                                   reinterpret_cast<cudaStream_t>(stream));
+    if (rc) return fail(rc, "giem2g_gemm_bf16_tn: bad shape or alignment (K, lda, ldb multiples of 8; 16-byte aligned A, B)");
+    return set_status(0);
+}
+
+int giem2g_im2col3d_bf16(const void *x, void *cols, int N, int D, int H, int W, int C, int stride, int Kp, void *stream)
+{
+    const int rc = ie_im2col3d(x, cols, N, D, H, W, C, stride, Kp, reinterpret_cast<cudaStream_t>(stream));
+    if (rc) return fail(rc, "giem2g_im2col3d_bf16: bad shape (stride 1 or 2, Kp >= 27C, Kp multiple of 8)");
+    return set_status(0);
+}
+
+int giem2g_col2im3d_f32(const float *dcols, float *dx, int N, int D, int H, int W, int C, int stride, int Kp,
+                        void *stream)
+{
+    const int rc = ie_col2im3d(dcols, dx, N, D, H, W, C, stride, Kp, reinterpret_cast<cudaStream_t>(stream));
+    if (rc) return fail(rc, "giem2g_col2im3d_f32: bad shape");
     return set_status(0);
 }
 

@@ -50,7 +50,7 @@ struct IeOp {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
     bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
-    int contract_variant[2] = {0, 0};  // tile-shape variant per precision (autotuner's pick)
+    int contract_variant[3] = {0, 0, 0};  // tile-shape variant: FP64, complex64, paired complex64
     // counters (Integral_Equation_Module.F90:44-56)
     long long mult_num = 0;
     double apply_seconds = 0;
@@ -82,10 +82,17 @@ int ie_apply_pair32(IeOp *op, const float2 *in0, const float2 *in1, float2 *out0
                     float2 *U1, float2 *Uh);
 bool ie_contract_pair32_supported(int Nx, int Ny, int Nz);
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
-                       const int *gate);
+                       const int *gate, int variant);
+int ie_contract_pair_variants(int Nz);
 // Process-wide static scratch of the static-scratch apply: device address (set-up on first use per
 // device) and capacity in bytes.
 int ie_static_scratch(void **ptr, size_t *capacity);
+// 3x3x3 convolution data movement (channels-last): im2col (bf16) and its gather-form adjoint (fp32)
+int ie_im2col3d(const void *x, void *cols, int N, int D, int H, int W, int C, int s, int Kp, cudaStream_t st);
+int ie_col2im3d(const float *dcols, float *dx, int N, int D, int H, int W, int C, int s, int Kp, cudaStream_t st);
+// BF16 tensor-core GEMM, FP32 out: C = A B^T (or C += A B^T), A [M][K], B [N][K] K-major
+int ie_gemm_bf16_tn(const void *A, const void *B, float *C, int M, int N, int K, int lda, int ldb, int ldc,
+                    int accumulate, int *err, cudaStream_t st);
 int ie_alloc_scratch(IeOp *op);
 int ie_make_twiddles(IeOp *op);
 int ie_kernel_launch_count_apply();

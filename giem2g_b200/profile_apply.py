@@ -21,7 +21,9 @@ def main(argv=None):
     ap.add_argument("--nz", type=int, default=32)
     ap.add_argument("--prec", type=int, default=0, choices=[0, 1])
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=0, help="untimed applies before the timed ones")
     ap.add_argument("--variant", type=int, default=None)
+    ap.add_argument("--nv", type=int, default=1, choices=[1, 2], help="vectors per apply (2: paired complex64)")
     args = ap.parse_args(argv)
     import torch
     import giem2g_b200 as g2
@@ -37,21 +39,31 @@ def main(argv=None):
     t_build = time.perf_counter() - t0
     op.set_anomaly_sigma(sig, m.freq)
     if args.variant is not None:
-        op.set_contract_variant(args.prec, args.variant)
+        op.set_contract_variant(2 if args.nv == 2 else args.prec, args.variant)
     dt = torch.complex128 if args.prec == 0 else torch.complex64
     g = torch.Generator(device="cuda").manual_seed(1)
     x = torch.randn(op.nvec, dtype=dt, device="cuda", generator=g)
     y = torch.empty_like(x)
     stream = torch.cuda.ExternalStream(op.stream)
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x2, y2 = torch.randn_like(x), torch.empty_like(x)
+
+    def one():
+        if args.nv == 2:
+            g2.apply_device_batch(op, [x.data_ptr(), x2.data_ptr()], [y.data_ptr(), y2.data_ptr()], args.prec)
+        else:
+            op.apply_device(x.data_ptr(), y.data_ptr(), args.prec)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.reps):
-        op.apply_device(x.data_ptr(), y.data_ptr(), args.prec)
+        one()
     e1.record(stream)
     torch.cuda.synchronize()
     op.check_device_error()
-    print(json.dumps({"grid": [Nx, Ny, Nz], "precision": args.prec, "reps": args.reps,
+    print(json.dumps({"grid": [Nx, Ny, Nz], "precision": args.prec, "nv": args.nv, "reps": args.reps,
                       "ms_per_apply": e0.elapsed_time(e1) / args.reps, "tensor_build_s": t_build}))
     op.delete()
 

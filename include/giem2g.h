@@ -110,7 +110,7 @@ int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_o
 int giem2g_check_device_error(void *ie);
 /* Contraction tile-shape variants available for a precision (0 or 1) at this Nz, and selection of one
  * (what the autotuner in giem2g_b200.autotune sets after timing them). */
-int giem2g_contract_variants(void *ie, int precision);
+int giem2g_contract_variants(void *ie, int precision);  /* precision 2: paired complex64 */
 int giem2g_set_contract_variant(void *ie, int precision, int variant);
 /* CUDA stream the operator's kernels run on (cudaStream_t). */
 void *giem2g_get_stream(void *ie);
@@ -170,6 +170,22 @@ void giem2g_batch_delete(void *batch);
  * reads, precision 0 one at a time. */
 int giem2g_apply_ie_operator_device_batch(void *ie, int nv, const void *const *d_in, void *const *d_out,
                                           int precision);
+
+/* ---- learned preconditioner building blocks (no counterpart in the reference) ----------------
+ * BF16 GEMM on the tcgen05 tensor cores with FP32 accumulation and output:
+ * C[M][N] = A[M][K] B[N][K]^T (accumulate 0) or C += A B^T (accumulate 1); A, B row-major bf16 with
+ * K contiguous; K, lda, ldb multiples of 8.  d_err: device int set nonzero if a bounded wait gave up
+ * (NULL: an internal one).  stream: cudaStream_t or NULL. */
+int giem2g_gemm_bf16_tn(const void *A, const void *B, float *C, int M, int N, int K, int lda, int ldb, int ldc,
+                        int accumulate, int *d_err, void *stream);
+/* 3x3x3 convolution with padding 1 and stride 1 or 2 on channels-last volumes x[N][D][H][W][C] (bf16):
+ * cols[N*Do*Ho*Wo][Kp] with column tap*C + c, tap = (dz*3 + dy)*3 + dx, zero beyond 27C (Kp >= 27C,
+ * multiple of 8); col2im is its adjoint, dx[N][D][H][W][C] (fp32) = sum of dcols over the taps that
+ * read each input element. */
+int giem2g_im2col3d_bf16(const void *x, void *cols, int N, int D, int H, int W, int C, int stride, int Kp,
+                         void *stream);
+int giem2g_col2im3d_f32(const float *dcols, float *dx, int N, int D, int H, int W, int C, int stride, int Kp,
+                        void *stream);
 
 #ifdef __cplusplus
 }
