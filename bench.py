@@ -259,6 +259,28 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.synchronize()
     fp64_pair_ms = ev0.elapsed_time(ev1)
 
+    # the learned outer preconditioner (trained on 64x64x16 C4 models) on the EY solve: warm start of the
+    # inner cycle (mode 1) and alone (mode 2, with the solver's fallback to the plain inner GMRES)
+    learned = None
+    try:
+        from giem2g_b200.learned import WEIGHTS, LearnedPreconditioner, UNet3D
+        if os.path.exists(WEIGHTS):
+            net = UNet3D.from_file(WEIGHTS)
+            pre = LearnedPreconditioner(net, m, sig)
+            learned = {"weights": os.path.relpath(WEIGHTS, ROOT)}
+            for label, mode in (("net_warm_start", 1), ("net_only_with_fallback", 2)):
+                pre.attach(op, mode)
+                op.solve_device(d_ey.data_ptr(), d_sol_y.data_ptr(), None, tol=TOL, max_restart=MAXRESTART,
+                                outer_buf=OUTER, inner_buf=INNER, precision=1)
+                li = op.solve_device(d_ey.data_ptr(), d_sol_y.data_ptr(), None, tol=TOL, max_restart=MAXRESTART,
+                                     outer_buf=OUTER, inner_buf=INNER, precision=1)
+                learned[label] = {"outer_iterations": li.iterations, "net_steps": li.precond_steps,
+                                  "ms": li.device_ms, "true_rel_residual": li.be}
+            op.set_outer_preconditioner(0)
+    except Exception as exc:  # reported, never the headline
+        learned = {"error": str(exc)}
+        op.set_outer_preconditioner(0)
+
     # mixed precision, one polarisation after the other (the reference's order); one untimed pair first
     # (work-space reallocation for the precision change, graph capture)
     solve_pair(1)
@@ -410,6 +432,7 @@ def run_b200(args, rank, world, local_rank):
                       "applies_mixed": [iy.applies_fp64 + iy.applies_fp32, ix.applies_fp64 + ix.applies_fp32],
                       "true_rel_residual_mixed": [iy.be, ix.be],
                       "field_error_vs_fp64_tol1e-8": [err_y, err_x]},
+            "learned_preconditioner": learned,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }

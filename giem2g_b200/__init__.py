@@ -49,6 +49,10 @@ class DataT(ctypes.Structure):            # giem2g_interfaces.F90:46-58
                 ("fft_buffer_in", ctypes.c_void_p), ("fft_buffer_out", ctypes.c_void_p)]
 
 
+PRECOND_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
+                              ctypes.c_void_p)
+
+
 class FgmresCtl(ctypes.Structure):        # data_types_module.F90:49-55 (+ precision)
     _fields_ = [("misfit", ctypes.c_double), ("fgmres_maxit", ctypes.c_int), ("gmres_buf", ctypes.c_int),
                 ("fgmres_buf", ctypes.c_int), ("precision", ctypes.c_int)]
@@ -57,7 +61,7 @@ class FgmresCtl(ctypes.Structure):        # data_types_module.F90:49-55 (+ preci
 class ResultT(ctypes.Structure):          # fgmres_interfaces.F90:34-39 (+ counters)
     _fields_ = [("iterations", ctypes.c_int), ("bea", ctypes.c_double), ("be", ctypes.c_double),
                 ("stat", ctypes.c_int), ("applies_fp64", ctypes.c_int), ("applies_fp32", ctypes.c_int),
-                ("device_ms", ctypes.c_double)]
+                ("device_ms", ctypes.c_double), ("precond_steps", ctypes.c_int)]
 
 
 EXPORTED_SYMBOLS = [
@@ -72,7 +76,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_apply_ie_operator_device_static", "giem2g_batch_create", "giem2g_batch_solve_device",
     "giem2g_solve_batched", "giem2g_batch_misfit_history", "giem2g_batch_delete",
     "giem2g_apply_ie_operator_device_batch", "giem2g_gemm_bf16_tn", "giem2g_im2col3d_bf16",
-    "giem2g_col2im3d_f32",
+    "giem2g_col2im3d_f32", "giem2g_set_outer_preconditioner", "giem2g_set_fft_lines",
 ]
 
 
@@ -137,6 +141,8 @@ def lib():
     L.giem2g_gemm_bf16_tn.argtypes = [vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, vp, vp]
     L.giem2g_im2col3d_bf16.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
     L.giem2g_col2im3d_f32.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
+    L.giem2g_set_outer_preconditioner.argtypes = [vp, ip, PRECOND_FN, vp]
+    L.giem2g_set_fft_lines.argtypes = [vp, ip]
     _lib = L
     return L
 
@@ -178,6 +184,7 @@ class SolveInfo:
     applies_fp32: int
     device_ms: float
     misfits: np.ndarray
+    precond_steps: int = 0
 
 
 class IEOperator:
@@ -276,6 +283,9 @@ class IEOperator:
     def set_contract_variant(self, precision: int, variant: int):
         _check(lib().giem2g_set_contract_variant(self.handle, precision, variant), "set_contract_variant")
 
+    def set_fft_lines(self, lines: int):
+        _check(lib().giem2g_set_fft_lines(self.handle, lines), "set_fft_lines")
+
     def check_device_error(self):
         _check(lib().giem2g_check_device_error(self.handle), "device error word")
 
@@ -295,7 +305,8 @@ class IEOperator:
     def _info(self, r):
         h = np.zeros(max(1, r.iterations), np.float64)
         n = lib().giem2g_get_misfit_history(self.handle, h.ctypes.data, len(h))
-        return SolveInfo(r.iterations, r.bea, r.be, r.stat, r.applies_fp64, r.applies_fp32, r.device_ms, h[:n].copy())
+        return SolveInfo(r.iterations, r.bea, r.be, r.stat, r.applies_fp64, r.applies_fp32, r.device_ms, h[:n].copy(),
+                         r.precond_steps)
 
     def solve_equation(self, E_bkg, E0=None, tol=1e-8, max_restart=100, outer_buf=30, inner_buf=10, precision=0):
         """SolveEquation with host arrays (Nx,Ny,Nz,3) complex128; returns (Esol, SolveInfo)."""
@@ -315,6 +326,24 @@ class IEOperator:
                                        self._ctl(tol, max_restart, outer_buf, inner_buf, precision), ctypes.byref(r))
         _check(rc, "giem2g_solve_device")
         return self._info(r)
+
+    def set_outer_preconditioner(self, mode, fn=None):
+        """giem2g_set_outer_preconditioner: fn(d_v, d_z, n, stream) -> 0 writes a guess of A^-1 v (mode 1:
+        warm start of the inner GMRES, mode 2: Z itself); mode 0 removes it."""
+        if mode == 0 or fn is None:
+            self._precond_ref = None
+            _check(lib().giem2g_set_outer_preconditioner(self.handle, 0, PRECOND_FN(), None), "set_outer_preconditioner")
+            return
+
+        def cb(user, d_v, d_z, n, stream):
+            try:
+                return int(fn(d_v, d_z, n, stream))
+            except Exception as exc:  # a failing hook is dropped for the rest of the solve
+                self._precond_error = exc
+                return 1
+        self._precond_ref = PRECOND_FN(cb)
+        _check(lib().giem2g_set_outer_preconditioner(self.handle, int(mode), self._precond_ref, None),
+               "set_outer_preconditioner")
 
     def print_stats(self):
         lib().giem2g_print_stats(self.handle)

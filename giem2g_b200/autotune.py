@@ -65,6 +65,27 @@ def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> di
         op.set_contract_variant(prec, best[0])
         picks[prec] = {"variant": best[0], "ms": best[1], "all_ms": all_ms}
         cache[ck] = picks[prec]
+    # FFT lines per CTA (one setting for both precisions), timed on the paired complex64 apply
+    x = torch.randn(op.nvec, dtype=torch.complex64, device="cuda")
+    x2, y, y2 = torch.randn_like(x), torch.empty_like(x), torch.empty_like(x)
+    best, all_ms = None, []
+    for lines in (32, 16, 8):
+        op.set_fft_lines(lines)
+        for _ in range(2):
+            apply_device_batch(op, [x.data_ptr(), x2.data_ptr()], [y.data_ptr(), y2.data_ptr()], 1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            apply_device_batch(op, [x.data_ptr(), x2.data_ptr()], [y.data_ptr(), y2.data_ptr()], 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        all_ms.append(round(ms, 5))
+        if best is None or ms < best[1]:
+            best = (lines, ms)
+    op.set_fft_lines(best[0])
+    picks["fft_lines"] = {"lines": best[0], "ms": best[1], "all_ms": all_ms}
     op.check_device_error()
     if cache_path:
         try:

@@ -305,9 +305,9 @@ template <> struct Bufs<float> {
 int ie_kernel_launch_count_apply() { return 5; }
 
 // lines per CTA: tile of at most ~100 KB of shared memory, power of two, <= 32
-static int lines_for(int L, size_t es)
+static int lines_for(int L, size_t es, int cap)
 {
-    int n = 32;
+    int n = cap >= 1 && cap <= 32 ? cap : 32;
     while (n > 1 && (size_t)(n * (L + 1) + L) * es > 100 * 1024) n >>= 1;
     return n;
 }
@@ -340,7 +340,7 @@ static void launch_x(bool fwd, IeOp *op, const VecSet<CT<R>> &vs, CT<R> *U1, cud
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = vs.nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
-    const int NL = lines_for(L, es), nt = threads_for(L, NL);
+    const int NL = lines_for(L, es, op->fft_lines), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
     dim3 grid((ZL + NL - 1) / NL, Ny);
     static bool attr = false;
@@ -357,7 +357,7 @@ static void launch_y(bool fwd, IeOp *op, int nv, CT<R> *U1, CT<R> *Uh, cudaStrea
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
-    const int NL = lines_for(L, es), nt = threads_for(L, NL);
+    const int NL = lines_for(L, es, op->fft_lines), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
     dim3 grid((ZL + NL - 1) / NL, 2 * Nx);
     static bool attr = false;

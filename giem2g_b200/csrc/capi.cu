@@ -381,6 +381,17 @@ int giem2g_set_contract_variant(void *ie, int precision, int variant)
     const int n = precision == 2 ? ie_contract_pair_variants(op->Nz) : ie_contract_variants(precision, op->Nz);
     if (variant < 0 || (variant > 0 && variant >= n)) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: variant %d of %d", variant, n);
     op->contract_variant[precision] = variant;
+    op->config_gen++;
+    return set_status(0);
+}
+
+int giem2g_set_fft_lines(void *ie, int lines)
+{
+    IeOp *op = resolve(ie);
+    if (!op || (lines != 4 && lines != 8 && lines != 16 && lines != 32))
+        return fail(G2_ERR_ARG, "giem2g_set_fft_lines: lines must be 4, 8, 16 or 32");
+    op->fft_lines = lines;
+    op->config_gen++;
     return set_status(0);
 }
 
@@ -574,6 +585,16 @@ int giem2g_col2im3d_f32(const float *dcols, float *dx, int N, int D, int H, int 
 {
     const int rc = ie_col2im3d(dcols, dx, N, D, H, W, C, stride, Kp, reinterpret_cast<cudaStream_t>(stream));
     if (rc) return fail(rc, "giem2g_col2im3d_f32: bad shape");
+    return set_status(0);
+}
+
+int giem2g_set_outer_preconditioner(void *ie, int mode, giem2g_precond_fn fn, void *user)
+{
+    IeOp *op = resolve(ie);
+    if (!op || mode < 0 || mode > 2 || (mode && !fn)) return fail(G2_ERR_ARG, "giem2g_set_outer_preconditioner: bad arguments");
+    op->precond_mode = mode;
+    op->precond_fn = mode ? fn : nullptr;
+    op->precond_user = mode ? user : nullptr;
     return set_status(0);
 }
 

@@ -28,6 +28,7 @@ constexpr int kVT = 256;   // threads of the vector kernels
 constexpr int KMAX = 32;   // largest basis handled in one sweep
 constexpr double ZERO_THRESHOLD = 1e-14;  // gmres.F90:21
 constexpr int N_IGS = 3;                  // gmres.F90:22
+constexpr double kHookGain = 0.5;         // an outer step through the hook must halve the misfit
 
 enum { F_KRYLOV = 0, F_PASS = 1, F_L = 2, F_ITER = 3, F_SOLVER = 4, F_NFLAGS = 8 };
 enum { S_BN = 0, S_BETA = 1, S_DNORMW = 2, S_DLOO = 3, S_BEA = 4, S_NRM2 = 5, S_NSCAL = 8 };
@@ -499,16 +500,19 @@ struct KrylovWork {
     // inner
     void *Vi = nullptr, *ri = nullptr, *wi = nullptr, *vin = nullptr, *xin = nullptr;
     Level Lo, Li;
-    // the inner GMRES cycle as a CUDA graph (fixed buffers vin -> xin), captured on its second use
-    cudaGraphExec_t inner_exec = nullptr;
-    double inner_tol = -1.0;
-    int inner_uses = 0, inner_graph_applies = 0, inner_graph_launches = 0;
-    bool inner_true_res = false;
-    int inner_cv[2] = {-1, -1};  // contraction variants baked into the captured graph
+    // the inner GMRES cycle as CUDA graphs (fixed buffers vin -> xin; slot 0 starts at x0 = vin as the
+    // reference does, slot 1 at x0 = x0in, the outer preconditioner hook's guess), captured on second use
+    cudaGraphExec_t inner_exec[2] = {nullptr, nullptr};
+    double inner_tol[2] = {-1.0, -1.0};
+    int inner_uses[2] = {0, 0}, inner_graph_applies[2] = {0, 0}, inner_graph_launches[2] = {0, 0};
+    bool inner_true_res[2] = {false, false};
+    long long inner_gen[2] = {-1, -1};          // operator launch configuration baked into the graphs
+    void *x0in = nullptr;                       // warm start of the inner cycle (inner precision)
     double2 *part = nullptr;
     int nparts = 0;
     std::vector<double> history;
     int applies64 = 0, applies32 = 0;
+    int hook_steps = 0;  // outer steps preconditioned through the hook in the last solve
 };
 
 static int alloc_level(Level &L, int m)
@@ -539,8 +543,9 @@ static void free_level(Level &L)
 static void kw_free(KrylovWork *k)
 {
     if (!k) return;
-    if (k->inner_exec) cudaGraphExecDestroy(k->inner_exec);
-    void *p[] = {k->Vo, k->x, k->b, k->r0, k->w, k->tmp, k->Zo, k->Vi, k->ri, k->wi, k->vin, k->xin, k->part};
+    for (int q = 0; q < 2; q++)
+        if (k->inner_exec[q]) cudaGraphExecDestroy(k->inner_exec[q]);
+    void *p[] = {k->Vo, k->x, k->b, k->r0, k->w, k->tmp, k->Zo, k->Vi, k->ri, k->wi, k->vin, k->xin, k->part, k->x0in};
     for (void *q : p)
         if (q) cudaFree(q);
     free_level(k->Lo);
@@ -574,6 +579,7 @@ static int kw_alloc(KrylovWork *k, size_t N, int mo, int mi, int precision)
     G2_CUDA_CHECK(cudaMalloc(&k->wi, ei * N));
     G2_CUDA_CHECK(cudaMalloc(&k->vin, ei * N));
     G2_CUDA_CHECK(cudaMalloc(&k->xin, ei * N));
+    G2_CUDA_CHECK(cudaMalloc(&k->x0in, ei * N));
     k->nparts = vec_grid(N);
     G2_CUDA_CHECK(cudaMalloc(&k->part, sizeof(double2) * (size_t)k->nparts * (KMAX + 1)));
     int rc = alloc_level(k->Lo, mo);
@@ -663,7 +669,8 @@ template <> int apply_prec<float2>(IeOp *op, const float2 *in, float2 *out, cuda
 
 // Inner GMRES (seq_fgmres.F90:142-152 -> gmres.F90:110-213 with MaxIt = 1, x0 = b = v): x = M(v)
 template <typename CI>
-static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, bool true_residual, cudaStream_t st)
+static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, const CI *x0, CI *x, double tol, bool true_residual,
+                       cudaStream_t st)
 {
     Level &L = k->Li;
     const size_t N = k->N;
@@ -673,8 +680,8 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
     k_zero_level<<<1, 256, 0, st>>>(L); g2_count_launches(1);
     norm2<CI>(k, v, L.scal + S_NRM2, nullptr, st);
     k_set_bn<<<1, 1, 0, st>>>(L); g2_count_launches(1);
-    k_copy_or_zero<CI><<<g, kVT, 0, st>>>(x, v, L.scal, N);  // x = x0, or 0 when ||b|| < 1e-14
-    int rc = apply_prec<CI>(op, v, ri, st, solver);
+    k_copy_or_zero<CI><<<g, kVT, 0, st>>>(x, x0, L.scal, N);  // x = x0, or 0 when ||b|| < 1e-14
+    int rc = apply_prec<CI>(op, x0, ri, st, solver);
     if (rc) return rc;
     k->applies32 += sizeof(CI) == 8 ? 1 : 0;
     k->applies64 += sizeof(CI) == 16 ? 1 : 0;
@@ -704,59 +711,61 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, CI *x, double tol, 
     return G2_OK;
 }
 
-// inner solve vin -> xin; eager on first use, then captured once and replayed as a CUDA graph
+// inner solve vin -> xin (warm: starting at x0in); eager on first use, then captured once and replayed
 template <typename CI>
-static int inner_solve_fixed(IeOp *op, KrylovWork *k, double tol, bool true_res, cudaStream_t st)
+static int inner_solve_fixed(IeOp *op, KrylovWork *k, double tol, bool true_res, bool warm, cudaStream_t st)
 {
+    const int q = warm ? 1 : 0;
     const CI *v = reinterpret_cast<const CI *>(k->vin);
+    const CI *x0 = warm ? reinterpret_cast<const CI *>(k->x0in) : v;
     CI *x = reinterpret_cast<CI *>(k->xin);
     const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
     const bool graphs = !(ng && ng[0] == '1');
-    if (k->inner_exec && (k->inner_tol != tol || k->inner_true_res != true_res ||
-                          k->inner_cv[0] != op->contract_variant[0] || k->inner_cv[1] != op->contract_variant[1])) {
-        cudaGraphExecDestroy(k->inner_exec);
-        k->inner_exec = nullptr;
-        k->inner_uses = 0;
+    if (k->inner_exec[q] && (k->inner_tol[q] != tol || k->inner_true_res[q] != true_res ||
+                             k->inner_gen[q] != op->config_gen)) {
+        cudaGraphExecDestroy(k->inner_exec[q]);
+        k->inner_exec[q] = nullptr;
+        k->inner_uses[q] = 0;
     }
-    if (k->inner_exec) {
-        G2_CUDA_CHECK(cudaGraphLaunch(k->inner_exec, st));
-        g2_count_launches(k->inner_graph_launches);
-        if (sizeof(CI) == 8) k->applies32 += k->inner_graph_applies;
-        else k->applies64 += k->inner_graph_applies;
+    auto credit = [&]() {
+        g2_count_launches(k->inner_graph_launches[q]);
+        if (sizeof(CI) == 8) k->applies32 += k->inner_graph_applies[q];
+        else k->applies64 += k->inner_graph_applies[q];
+    };
+    if (k->inner_exec[q]) {
+        G2_CUDA_CHECK(cudaGraphLaunch(k->inner_exec[q], st));
+        credit();
         return G2_OK;
     }
-    if (!graphs || k->inner_uses++ == 0) return inner_solve<CI>(op, k, v, x, tol, true_res, st);
+    if (!graphs || k->inner_uses[q]++ == 0) return inner_solve<CI>(op, k, v, x0, x, tol, true_res, st);
     // capture: count what one cycle launches, then instantiate
     const int a32 = k->applies32, a64 = k->applies64;
     const long long l0 = g2_launch_total();
     cudaGraph_t graph = nullptr;
     G2_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    int rc = inner_solve<CI>(op, k, v, x, tol, true_res, st);
+    int rc = inner_solve<CI>(op, k, v, x0, x, tol, true_res, st);
     cudaError_t ce = cudaStreamEndCapture(st, &graph);
     if (rc) return rc;
     if (ce != cudaSuccess) {
         g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
         return G2_ERR_CUDA;
     }
-    k->inner_graph_applies = (k->applies32 - a32) + (k->applies64 - a64);
-    k->inner_graph_launches = (int)(g2_launch_total() - l0);
+    k->inner_graph_applies[q] = (k->applies32 - a32) + (k->applies64 - a64);
+    k->inner_graph_launches[q] = (int)(g2_launch_total() - l0);
     k->applies32 = a32;
     k->applies64 = a64;
-    ce = cudaGraphInstantiate(&k->inner_exec, graph, 0);
+    ce = cudaGraphInstantiate(&k->inner_exec[q], graph, 0);
     cudaGraphDestroy(graph);
     if (ce != cudaSuccess) {
         g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
-        k->inner_exec = nullptr;
+        k->inner_exec[q] = nullptr;
         return G2_ERR_CUDA;
     }
-    k->inner_tol = tol;
-    k->inner_true_res = true_res;
-    k->inner_cv[0] = op->contract_variant[0];
-    k->inner_cv[1] = op->contract_variant[1];
-    G2_CUDA_CHECK(cudaGraphLaunch(k->inner_exec, st));
-    g2_count_launches(k->inner_graph_launches);
-    if (sizeof(CI) == 8) k->applies32 += k->inner_graph_applies;
-    else k->applies64 += k->inner_graph_applies;
+    k->inner_tol[q] = tol;
+    k->inner_true_res[q] = true_res;
+    k->inner_gen[q] = op->config_gen;
+    G2_CUDA_CHECK(cudaGraphLaunch(k->inner_exec[q], st));
+    credit();
     return G2_OK;
 }
 
@@ -809,7 +818,8 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
         return G2_OK;
     }
     int iter = 0, L_used = 0;
-    bool converged = false;
+    bool converged = false, hook_off = false;
+    k->hook_steps = 0;
     double bea = -1.0;
     char msg[256];
     for (;;) {
@@ -819,10 +829,25 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
             const double2 *Vj = k->Vo + (size_t)j * N;
             CI *Zj = Z + (size_t)j * N;
             // right preconditioner: Z_j = inner GMRES(V_j)  (gmres.F90:251, :491-506), through the fixed
-            // buffers vin -> xin of the captured inner cycle
-            k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(vin, 1.0, Vj, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
-            if ((rc = inner_solve_fixed<CI>(op, k, tol, true_res, st))) return rc;
-            k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, N, nullptr); g2_count_launches(1);
+            // buffers vin -> xin of the captured inner cycle.  With an outer preconditioner hook the hook's
+            // output (complex128 in tmp) either starts the inner cycle (mode 1) or is Z_j itself (mode 2).
+            bool hooked = false;
+            if (op->precond_mode && !hook_off) {
+                const int hr = op->precond_fn(op->precond_user, Vj, k->tmp, (long long)N, reinterpret_cast<void *>(st));
+                if (hr == 0) hooked = true;
+                else hook_off = true;
+            }
+            if (hooked && op->precond_mode == 2) {
+                k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(Zj, 1.0, k->tmp, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
+            } else {
+                k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(vin, 1.0, Vj, 0.0, (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
+                if (hooked) {
+                    k_axpby<CI, double2, double2><<<g, kVT, 0, st>>>(reinterpret_cast<CI *>(k->x0in), 1.0, k->tmp, 0.0,
+                                                                     (const double2 *)nullptr, N, nullptr); g2_count_launches(1);
+                }
+                if ((rc = inner_solve_fixed<CI>(op, k, tol, true_res, hooked, st))) return rc;
+                k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, N, nullptr); g2_count_launches(1);
+            }
             if (sizeof(CI) == sizeof(double2)) {
                 if ((rc = ie_apply_device64(op, reinterpret_cast<const double2 *>(Zj), k->w, st))) return rc;
             } else {
@@ -838,6 +863,9 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
                 g2_set_error_msg("FGMRES: non-finite Arnoldi misfit");
                 return G2_ERR_NUMERIC;
             }
+            // the hook must keep reducing the FP64 residual; otherwise the plain inner GMRES takes over
+            if (hooked && !k->history.empty() && !(bea < kHookGain * k->history.back())) hook_off = true;
+            if (hooked) k->hook_steps++;
             k->history.push_back(bea);
             info->iterations = (int)k->history.size();
             // ie_solver_module.F90:335-343 Information
@@ -915,6 +943,7 @@ int krylov_solve_device(IeOp *op, const double2 *d_Ebkg, double2 *d_Esol, const 
     cudaEventDestroy(e1);
     info->applies_fp64 = k->applies64;
     info->applies_fp32 = k->applies32;
+    info->precond_steps = k->hook_steps;
     info->device_ms = ms;
     op->mult_num += k->applies64 + k->applies32;
     op->apply_seconds += ms * 1e-3;
@@ -970,7 +999,8 @@ struct BatchWork {
     cudaGraphExec_t inner_exec = nullptr;
     double inner_tol = -1.0;
     int inner_uses = 0, inner_graph_launches = 0;
-    std::vector<int> inner_graph_applies, cv;
+    std::vector<int> inner_graph_applies;
+    std::vector<long long> cv;
     std::vector<std::vector<double>> history;
 };
 
@@ -1133,9 +1163,8 @@ static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
         G2_CUDA_CHECK(cudaMemcpyAsync(b->d_active, b->h_active.data(), sizeof(int) * b->n, cudaMemcpyHostToDevice, st));
         b->dev_active = b->h_active;
     }
-    std::vector<int> cv;
-    for (IeOp *op : b->ops)
-        for (int q = 0; q < 3; q++) cv.push_back(op->contract_variant[q]);
+    std::vector<long long> cv;
+    for (IeOp *op : b->ops) cv.push_back(op->config_gen);
     const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
     const bool graphs = !(ng && ng[0] == '1');
     if (b->inner_exec && (b->inner_tol != tol || b->cv != cv)) {

@@ -112,6 +112,8 @@ int giem2g_check_device_error(void *ie);
  * (what the autotuner in giem2g_b200.autotune sets after timing them). */
 int giem2g_contract_variants(void *ie, int precision);  /* precision 2: paired complex64 */
 int giem2g_set_contract_variant(void *ie, int precision, int variant);
+/* Lines per CTA of the FFT passes (4, 8, 16 or 32; default 32), also set by the autotuner. */
+int giem2g_set_fft_lines(void *ie, int lines);
 /* CUDA stream the operator's kernels run on (cudaStream_t). */
 void *giem2g_get_stream(void *ie);
 /* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */
@@ -136,6 +138,7 @@ typedef struct {
     int applies_fp64;
     int applies_fp32;
     double device_ms;
+    int precond_steps;   /* outer steps preconditioned through the outer preconditioner hook */
 } GIEM2G_RESULT;
 
 /* SolveEquation (ie_solver_module.F90:43-114): E_bkg, Esol, E0 host arrays (Nx,Ny,Nz,3)
@@ -147,6 +150,15 @@ int giem2g_solve_device(void *ie, const void *d_E_bkg, void *d_Esol, const void 
                         GIEM2G_RESULT *info);
 /* Outer Arnoldi misfit after each outer iteration of the last solve; returns the count copied. */
 int giem2g_get_misfit_history(void *ie, double *out, int max_len);
+/* Outer right preconditioner hook (no counterpart in the reference; the learned preconditioner).
+ * fn(user, d_v, d_z, n, stream) receives V_j (complex128, n elements, device) and writes its guess of
+ * A^-1 V_j to d_z (complex128, device) on `stream`, returning 0 (nonzero: the hook is dropped for the
+ * rest of the solve).  mode 1: the guess starts the inner GMRES cycle (x0 = guess instead of x0 = V_j);
+ * mode 2: the guess is Z_j itself (no inner cycle); mode 0 removes the hook.  Whenever an outer step
+ * through the hook fails to halve the Arnoldi misfit, the plain inner GMRES takes over for the rest of
+ * the solve.  Single-instance solves only (giem2g_solve, giem2g_solve_device). */
+typedef int (*giem2g_precond_fn)(void *user, const void *d_v, void *d_z, long long n, void *stream);
+int giem2g_set_outer_preconditioner(void *ie, int mode, giem2g_precond_fn fn, void *user);
 
 /* ---- batched solves -----------------------------------------------------------
  * The reference solves one (frequency, polarisation) after another (giem2g.F90:336-373).  A batch

@@ -1,0 +1,200 @@
+"""Learned outer preconditioner: the convolution layers (forward and both gradients) against a plain
+PyTorch FP64 CPU reference, the network gradient against the same reference, and the solver hook.
+
+Tolerances: a layer sees BF16-rounded inputs, weights and upstream gradients on both sides, so the only
+difference is FP32 accumulation: 1e-5 relative.  Through the whole network the reference rounds to BF16
+where the GPU does, but an accumulation-order difference can flip a BF16 rounding and later layers carry
+it: output within 1e-2, every weight gradient within 5e-2 and cosine similarity > 0.998.
+"""
+import numpy as np
+import pytest
+
+from giem2g_b200.sources import plane_wave_integral
+from giem2g_b200.synthetic import config_c4
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf(t):
+    import torch
+    return t.to(torch.bfloat16).to(torch.float64)
+
+
+def _torch_w(w, cin):
+    """[Cout, Kp] (column tap*C + c) -> [Cout, C, 3, 3, 3]"""
+    cout = w.shape[0]
+    return w[:, :27 * cin].reshape(cout, 3, 3, 3, cin).permute(0, 4, 1, 2, 3)
+
+
+@pytest.mark.parametrize("stride", [1, 2])
+def test_conv3d_layer_vs_cpu(g2lib, stride):
+    import torch
+    import torch.nn.functional as F
+    from giem2g_b200.learned import _kp, conv3d
+    g = torch.Generator().manual_seed(3 + stride)
+    N, D, H, W, C, cout = 2, 4, 6, 8, 12, 16
+    x = torch.randn(N, D, H, W, C, generator=g)
+    w = torch.zeros(cout, _kp(C))
+    w[:, :27 * C] = torch.randn(cout, 27 * C, generator=g) * 0.1
+    xg = x.cuda().requires_grad_(True)
+    wg = w.cuda().requires_grad_(True)
+    y = conv3d(xg, wg, stride)
+    gy = torch.randn(y.shape, generator=g)
+    y.backward(gy.cuda())
+    # reference on the same bf16-rounded operands, FP64 on the CPU
+    xr = _bf(x).permute(0, 4, 1, 2, 3).requires_grad_(True)
+    wr = _bf(_torch_w(w, C)).requires_grad_(True)
+    yr = F.conv3d(xr, wr, stride=stride, padding=1)
+    yr.backward(_bf(gy).permute(0, 4, 1, 2, 3))
+    rel = lambda a, b: float((a - b).norm() / b.norm())
+    assert rel(y.detach().cpu().double().permute(0, 4, 1, 2, 3), yr.detach()) < 1e-5
+    assert rel(xg.grad.cpu().double().permute(0, 4, 1, 2, 3), xr.grad) < 1e-5
+    assert rel(_torch_w(wg.grad.cpu().double(), C), wr.grad) < 1e-5
+    if wg.grad.shape[1] > 27 * C:  # padding columns of the weight matrix get no gradient
+        assert float(wg.grad[:, 27 * C:].abs().max()) == 0.0
+
+
+def _cpu_conv_fn():
+    """FP64 CPU convolution that rounds its input, weight and upstream gradient to BF16 exactly where the
+    GPU layer does; only the accumulation precision differs."""
+    import torch
+    import torch.nn.functional as F
+
+    class RefConv(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, x, w, stride):  # x: [N, C, D, H, W], w: [Cout, C, 3, 3, 3]
+            xb, wb = _bf(x), _bf(w)
+            ctx.save_for_backward(xb, wb)
+            ctx.stride = stride
+            return F.conv3d(xb, wb, stride=stride, padding=1)
+
+        @staticmethod
+        def backward(ctx, dy):
+            xb, wb = ctx.saved_tensors
+            dyb = _bf(dy)
+            dx = torch.nn.grad.conv3d_input(xb.shape, wb, dyb, stride=ctx.stride, padding=1)
+            dw = torch.nn.grad.conv3d_weight(xb, wb.shape, dyb, stride=ctx.stride, padding=1)
+            return dx, dw, None
+
+    return RefConv
+
+
+def test_unet_gradient_vs_cpu(g2lib):
+    import torch
+    from giem2g_b200.learned import CIN, UNet3D, _up
+    net = UNet3D(seed=5)
+    g = torch.Generator().manual_seed(11)
+    x = torch.randn(1, 16, 16, 16, CIN, generator=g)
+    out = net(x.cuda())
+    loss = (out ** 2).sum()
+    loss.backward()
+    ref = _cpu_conv_fn()
+    ws = {k: _torch_w(v.detach().cpu().double(), cin).clone().requires_grad_(True)
+          for (k, v), cin in zip(net.w.items(), [c for _, c, _, _ in UNet3D.LAYERS])}
+
+    def c(name, t, relu=True):
+        y = ref.apply(t.permute(0, 4, 1, 2, 3), ws[name], net.stride[name]).permute(0, 2, 3, 4, 1)
+        return torch.relu(y) if relu else y
+    xr = x.double()
+    e0 = c("e0", c("in", xr))
+    e1 = c("e1", c("d1", e0))
+    e2 = c("e2", c("d2", e1))
+    b = c("b", c("d3", e2))
+    u2 = c("u2", torch.cat([_up(b), e2], -1))
+    u1 = c("u1", torch.cat([_up(u2), e1], -1))
+    u0 = c("u0", torch.cat([_up(u1), e0], -1))
+    outr = c("out", u0, relu=False)[..., :6]
+    (outr ** 2).sum().backward()
+    # a different FP32 accumulation order can move a value across a BF16 rounding boundary (2^-8), and
+    # the next layer carries that difference on, so the bounds are set by BF16 resolution
+    out_err = float((out.detach().cpu().double() - outr.detach()).norm() / outr.norm())
+    assert out_err < 1e-2
+    for (k, wgpu), (name, cin, _, _) in zip(net.w.items(), UNet3D.LAYERS):
+        a = _torch_w(wgpu.grad.cpu().double(), cin).flatten()
+        r = ws[k].grad.flatten()
+        rel, cos = float((a - r).norm() / r.norm()), float(a @ r / (a.norm() * r.norm()))
+        print(f"layer {k}: gradient rel. error {rel:.2e}, cosine {cos:.6f}")
+        assert rel < 5e-2 and cos > 0.998, k
+
+
+def _c4_op(g2, seed):
+    m, sig = config_c4(seed=seed)
+    op = g2.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    op.calc_fft_of_ie_kernel()
+    op.set_anomaly_sigma(sig, m.freq)
+    return m, sig, op
+
+
+def test_hook_identity_reproduces_plain_solve(g2lib):
+    """mode 1 with guess z = v starts the inner cycle exactly where the reference starts it"""
+    import torch
+    m, sig, op = _c4_op(g2lib, 901)
+    b = torch.from_numpy(np.ascontiguousarray(plane_wave_integral(m, 1)).ravel()).cuda()
+    y0, y1 = torch.empty_like(b), torch.empty_like(b)
+    i0 = op.solve_device(b.data_ptr(), y0.data_ptr(), None, tol=1e-8, precision=1)
+
+    def ident(d_v, d_z, n, stream):
+        from giem2g_b200.learned import _DevView
+        with torch.cuda.stream(torch.cuda.ExternalStream(int(stream))):
+            torch.as_tensor(_DevView(d_z, n), device="cuda").copy_(torch.as_tensor(_DevView(d_v, n), device="cuda"))
+        return 0
+    op.set_outer_preconditioner(1, ident)
+    i1 = op.solve_device(b.data_ptr(), y1.data_ptr(), None, tol=1e-8, precision=1)
+    op.set_outer_preconditioner(0)
+    torch.cuda.synchronize()
+    assert i1.iterations == i0.iterations and i1.stat == i0.stat == 1
+    assert i1.precond_steps == i1.iterations
+    assert float((y1 - y0).norm() / y0.norm()) < 1e-12
+    op.delete()
+
+
+def test_hook_fallback_on_useless_guess(g2lib):
+    """a hook that does not reduce the residual is dropped and the plain inner GMRES finishes the solve"""
+    import torch
+    m, sig, op = _c4_op(g2lib, 902)
+    b = torch.from_numpy(np.ascontiguousarray(plane_wave_integral(m, 0)).ravel()).cuda()
+    y = torch.empty_like(b)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+
+    def noise(d_v, d_z, n, stream):
+        from giem2g_b200.learned import _DevView
+        with torch.cuda.stream(torch.cuda.ExternalStream(int(stream))):
+            torch.as_tensor(_DevView(d_z, n), device="cuda").copy_(
+                torch.randn(n, dtype=torch.complex128, device="cuda", generator=gen))
+        return 0
+    op.set_outer_preconditioner(2, noise)
+    info = op.solve_device(b.data_ptr(), y.data_ptr(), None, tol=1e-8, precision=1)
+    op.set_outer_preconditioner(0)
+    assert info.stat == 1 and info.be < 1e-8
+    assert info.precond_steps <= 2
+    op.delete()
+
+
+def test_trained_network_gain(g2lib):
+    """What the committed, trained network gains on unseen C4 models: its guess of A^-1 v against the
+    guess z = v of the plain method, and the outer iterations of solves that use it."""
+    import os
+    import torch
+    from giem2g_b200.learned import WEIGHTS, LearnedPreconditioner, UNet3D, evaluate, make_pairs
+    assert os.path.exists(WEIGHTS)
+    net = UNet3D.from_file(WEIGHTS)
+    X, Y = make_pairs(n_models=2, pairs_per_model=2, seed=99, solve_pairs=False, log=None)
+    err = evaluate(net, X, Y)
+    assert err < 0.5  # squared error of the correction, relative to the plain guess's (1.0)
+    m, sig, op = _c4_op(g2lib, 903)
+    b = torch.from_numpy(np.ascontiguousarray(plane_wave_integral(m, 1)).ravel()).cuda()
+    y = torch.empty_like(b)
+    plain = op.solve_device(b.data_ptr(), y.data_ptr(), None, tol=1e-6, precision=1)
+    pre = LearnedPreconditioner(net, m, sig)
+    pre.attach(op, 1)
+    warm = op.solve_device(b.data_ptr(), y.data_ptr(), None, tol=1e-6, precision=1)
+    pre.attach(op, 2)
+    only = op.solve_device(b.data_ptr(), y.data_ptr(), None, tol=1e-6, precision=1)
+    op.set_outer_preconditioner(0)
+    print(f"correction error {err:.3f}; outer iterations plain {plain.iterations}, net warm start "
+          f"{warm.iterations}, net only {only.iterations} ({only.precond_steps} net steps)")
+    assert plain.stat == warm.stat == only.stat == 1
+    assert warm.iterations <= plain.iterations + 1
+    assert only.precond_steps <= 2 and only.iterations <= plain.iterations + 3
+    op.delete()
