@@ -993,7 +993,7 @@ struct BatchWork {
     std::vector<KrylovWork *> k;
     std::vector<BatchGroup> groups;
     int *d_active = nullptr;
-    std::vector<int> h_active, dev_active;
+    std::vector<int> h_active, dev_active, graph_active;  // host mask, copy on the device, mask of the graph
     double2 *d_stage = nullptr;  // host-array solves: E_bkg[n] then E_sol[n] (complex128)
     cudaStream_t st = nullptr;
     cudaGraphExec_t inner_exec = nullptr;
@@ -1072,7 +1072,8 @@ template <typename CI, typename FIn, typename FOut>
 static int batch_apply(BatchWork *b, FIn in, FOut out, int flag, cudaStream_t st)
 {
     for (const BatchGroup &g : b->groups) {
-        if (g.n == 2 && sizeof(CI) == sizeof(float2)) {
+        const bool both = g.n == 2 && b->h_active[g.first] && b->h_active[g.first + 1];
+        if (both && sizeof(CI) == sizeof(float2)) {
             float2 *U1 = nullptr, *Uh = nullptr;
             int rc = ie_pair_scratch(g.op, &U1, &Uh);
             if (rc) return rc;
@@ -1088,6 +1089,7 @@ static int batch_apply(BatchWork *b, FIn in, FOut out, int flag, cudaStream_t st
             if (rc != G2_ERR_UNSUPPORTED) return rc;
         }
         for (int i = g.first; i < g.first + g.n; i++) {
+            if (!b->h_active[i]) continue;
             const int rc = apply_prec<CI>(g.op, in(i), out(i), st, b->k[i]->Li.flags + flag);
             if (rc) return rc;
             if (sizeof(CI) == sizeof(float2)) b->k[i]->applies32++;
@@ -1103,6 +1105,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
 {
     const int n = b->n;
     for (int i = 0; i < n; i++) {
+        if (!b->h_active[i]) continue;
         KrylovWork *k = b->k[i];
         Level &L = k->Li;
         const int g = vec_grid(k->N);
@@ -1117,6 +1120,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
     int rc = batch_apply<CI>(b, vin, ri, F_SOLVER, st);
     if (rc) return rc;
     for (int i = 0; i < n; i++) {
+        if (!b->h_active[i]) continue;
         KrylovWork *k = b->k[i];
         Level &L = k->Li;
         const int g = vec_grid(k->N);
@@ -1133,6 +1137,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         auto wi = [&](int i) { return reinterpret_cast<CI *>(b->k[i]->wi); };
         if ((rc = batch_apply<CI>(b, vj, wi, F_KRYLOV, st))) return rc;
         for (int i = 0; i < n; i++) {
+            if (!b->h_active[i]) continue;
             KrylovWork *k = b->k[i];
             Level &L = k->Li;
             const int g = vec_grid(k->N);
@@ -1143,6 +1148,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         }
     }
     for (int i = 0; i < n; i++) {
+        if (!b->h_active[i]) continue;
         KrylovWork *k = b->k[i];
         Level &L = k->Li;
         const int g = vec_grid(k->N);
@@ -1167,7 +1173,7 @@ static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
     for (IeOp *op : b->ops) cv.push_back(op->config_gen);
     const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
     const bool graphs = !(ng && ng[0] == '1');
-    if (b->inner_exec && (b->inner_tol != tol || b->cv != cv)) {
+    if (b->inner_exec && (b->inner_tol != tol || b->cv != cv || b->graph_active != b->h_active)) {
         cudaGraphExecDestroy(b->inner_exec);
         b->inner_exec = nullptr;
         b->inner_uses = 0;
@@ -1213,6 +1219,7 @@ static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
     }
     b->inner_tol = tol;
     b->cv = cv;
+    b->graph_active = b->h_active;
     G2_CUDA_CHECK(cudaGraphLaunch(b->inner_exec, st));
     credit();
     return G2_OK;

@@ -24,6 +24,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=0, help="untimed applies before the timed ones")
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--nv", type=int, default=1, choices=[1, 2], help="vectors per apply (2: paired complex64)")
+    ap.add_argument("--fft-lines", type=int, default=None, choices=[4, 8, 16, 32], help="lines per CTA of the FFTs")
     args = ap.parse_args(argv)
     import torch
     import giem2g_b200 as g2
@@ -40,6 +41,8 @@ def main(argv=None):
     op.set_anomaly_sigma(sig, m.freq)
     if args.variant is not None:
         op.set_contract_variant(2 if args.nv == 2 else args.prec, args.variant)
+    if args.fft_lines is not None:
+        op.set_fft_lines(args.fft_lines)
     dt = torch.complex128 if args.prec == 0 else torch.complex64
     g = torch.Generator(device="cuda").manual_seed(1)
     x = torch.randn(op.nvec, dtype=dt, device="cuda", generator=g)

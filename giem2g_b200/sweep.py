@@ -5,6 +5,7 @@ the Green's tensor, transform it, set the anomaly, solve EY then EX), with the i
 batch (giem2g_batch_*): every (frequency, polarisation) instance runs its own nested FGMRES, in
 lockstep with the others, and the two polarisations of one frequency share each complex64 tensor read.
 
+    python -m giem2g_b200.sweep --config c1 --precision 0 --tol 1e-8   # 32x32x8 block model, FP64
     python -m giem2g_b200.sweep --config c3            # 128x128x32, 8 frequencies x 2 polarisations
     python -m giem2g_b200.sweep --config c5 --compare  # 256x256x48 + ellipsoids, 4 x 2, vs sequential
 
@@ -22,7 +23,10 @@ import numpy as np
 
 
 def sweep_config(name: str):
-    from .synthetic import config_c2, config_c5
+    from .synthetic import config_c2, config_c5, config_small_block
+    if name == "c1":
+        m, sig = config_small_block()
+        return m, sig, [1.0]
     if name == "c3":
         m, sig = config_c2(seed=2024)
         return m, sig, list(np.logspace(-3, 2, 8))
@@ -54,6 +58,15 @@ def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner
         setup_s.append(time.perf_counter() - t0)
         ops.append((mf, op))
     out["setup_s_per_frequency"] = setup_s
+    # tile shapes: time the variants on the first operator; the others have the same grid
+    from .autotune import autotune_contraction
+    tuned = autotune_contraction(ops[0][1])
+    for _, op in ops[1:]:
+        for prec in (0, 1, 2):
+            if str(prec) in tuned and op.contract_variants(prec) > 1:
+                op.set_contract_variant(prec, tuned[str(prec)]["variant"])
+        op.set_fft_lines(tuned["fft_lines"]["lines"])
+    out["tuned"] = tuned
     inst_ops, d_rhs = [], []
     for mf, op in ops:
         for p in pols:
@@ -67,6 +80,7 @@ def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner
                       "iterations": [i.iterations for i in infos], "stat": [i.stat for i in infos],
                       "true_rel_residual": [i.be for i in infos],
                       "applies": [i.applies_fp64 + i.applies_fp32 for i in infos]}
+    batch.delete()  # its work space goes before the sequential solves allocate theirs
     if compare:
         for label, prec, t in (("sequential_mixed", 1, tol), ("sequential_fp64", 0, tol)):
             ms, its = 0.0, []
@@ -88,7 +102,6 @@ def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner
         out["field_error_vs_fp64"] = errs
         out["speedup_batched_vs_sequential_fp64"] = out["sequential_fp64"]["device_ms"] / out["batched"]["device_ms"]
         out["speedup_batched_vs_sequential_mixed"] = out["sequential_mixed"]["device_ms"] / out["batched"]["device_ms"]
-    batch.delete()
     for _, op in ops:
         op.delete()
     return out
@@ -96,7 +109,7 @@ def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", default="c3", choices=["c2", "c3", "c5"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c5"])
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
     ap.add_argument("--compare", action="store_true")
