@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
 // with the broadcast pairs (u.x, u.x), (u.y, u.y) prepared once per unit in shared memory.  Per j a thread
 // issues 8 tensor loads, 24 broadcast loads and 72 packed FMAs (144 FMAs).
 // Threads (b, v, s, z): unit b of the stage, vector v (NP vectors share the tensor), j-slice s, row z.
-template <int NZ, int S, int B, int NSTAGE, int NP>
+template <int NZ, int S, int B, int NSTAGE, int NP, int MINB = 1>
 struct CfgW {
     static constexpr int P = NZ * (NZ + 1) / 2;
     static constexpr int T = 4 * P + 2 * NZ * NZ;
@@ -252,6 +252,7 @@ struct CfgW {
     static_assert(RED_BYTES <= TBYTES, "reduction buffer reuses the drained tensor stage");
     static_assert(STAGE_BYTES % 16 == 0 && TBYTES % 16 == 0, "bulk copies need 16-byte multiples");
     static_assert(SMEM <= 232448, "exceeds the 227 KB dynamic shared memory of one CTA");
+    static_assert(MINB * (SMEM + 1024) <= 233472, "MINB CTAs do not fit the SM's shared memory");
 };
 
 G2_D float2 ffma2(float2 a, float2 b, float2 c)
@@ -264,13 +265,13 @@ G2_D float2 ffma2(float2 a, float2 b, float2 c)
     return ud.f;
 }
 
-template <int NZ, int S, int B, int NSTAGE, int NP>
-__global__ void __launch_bounds__(CfgW<NZ, S, B, NSTAGE, NP>::NTHREADS, 1)
+template <int NZ, int S, int B, int NSTAGE, int NP, int MINB>
+__global__ void __launch_bounds__(CfgW<NZ, S, B, NSTAGE, NP, MINB>::NTHREADS, MINB)
     k_contract_w32(const float2 *__restrict__ G, float2 *__restrict__ Uhat, int Ny, long long nbatches, int *err,
                    const int *gate)
 {
     if (gate && *gate == 0) return;
-    using Cfg = CfgW<NZ, S, B, NSTAGE, NP>;
+    using Cfg = CfgW<NZ, S, B, NSTAGE, NP, MINB>;
     constexpr int PTS = Cfg::PTS, Z3 = Cfg::Z3;
     constexpr int AW = asw_width32(NZ);
     extern __shared__ __align__(128) unsigned char smem[];
@@ -457,11 +458,12 @@ __global__ void __launch_bounds__(CfgW<NZ, S, B, NSTAGE, NP>::NTHREADS, 1)
     }
 }
 
-template <int NZ, int S, int B, int NSTAGE, int NP>
+template <int NZ, int S, int B, int NSTAGE, int NP, int MINB = 1>
 int launch_w32(const float2 *G, float2 *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
-    using Cfg = CfgW<NZ, S, B, NSTAGE, NP>;
-    auto kern = k_contract_w32<NZ, S, B, NSTAGE, NP>;
+    using Cfg = CfgW<NZ, S, B, NSTAGE, NP, MINB>;
+    auto kern = k_contract_w32<NZ, S, B, NSTAGE, NP, MINB>;
+    nsm *= MINB;
     static bool attr = false;
     if (!attr) {
         G2_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
@@ -515,8 +517,8 @@ int sm_count()
 // on the operator's own buffers and stores its pick in the operator.
 int ie_contract_variants(int precision, int Nz)
 {
-    if (precision == 0) return Nz == 32 ? 4 : (Nz == 8 || Nz == 16 ? 1 : 0);
-    return Nz == 32 ? 11 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    if (precision == 0) return Nz == 32 ? 4 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
+    return Nz == 32 ? 12 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
@@ -527,6 +529,7 @@ int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, 
     switch (Nz) {
     case 8: return launch_cfg<double, 8, 2, 8, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 16: return launch_cfg<double, 16, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 48: return launch_cfg<double, 48, 4, 1, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 32:
         if (v == 1) return launch_cfg<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 2) return launch_cfg<double, 32, 4, 1, 1, 1, false, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
@@ -559,6 +562,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         case 8: return launch_cfg<float, 32, 4, 1, 2, 1, false, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 9: return launch_cfg<float, 32, 2, 1, 1, 1, false, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 10: return launch_cfg<float, 32, 2, 1, 2, 1, false, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 11: return launch_w32<32, 4, 1, 2, 1, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         default: return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
         }
     case 48:
@@ -572,7 +576,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 7 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 8 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -593,6 +597,7 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         if (v == 4) return launch_cfg<float, 32, 4, 1, 2, 2, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 5) return launch_cfg<float, 32, 4, 1, 2, 2, false, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 6) return launch_cfg<float, 32, 2, 1, 1, 2, true, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 7) return launch_w32<32, 4, 1, 2, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 32, 4, 2, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
