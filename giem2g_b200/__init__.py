@@ -77,6 +77,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_solve_batched", "giem2g_batch_misfit_history", "giem2g_batch_delete",
     "giem2g_apply_ie_operator_device_batch", "giem2g_gemm_bf16_tn", "giem2g_im2col3d_bf16",
     "giem2g_col2im3d_f32", "giem2g_set_outer_preconditioner", "giem2g_set_fft_lines",
+    "giem2g_set_kernel_timing", "giem2g_last_contract_ms",
 ]
 
 
@@ -143,6 +144,9 @@ def lib():
     L.giem2g_col2im3d_f32.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
     L.giem2g_set_outer_preconditioner.argtypes = [vp, ip, PRECOND_FN, vp]
     L.giem2g_set_fft_lines.argtypes = [vp, ip]
+    L.giem2g_set_kernel_timing.argtypes = [vp, ip]
+    L.giem2g_last_contract_ms.argtypes = [vp]
+    L.giem2g_last_contract_ms.restype = dp
     _lib = L
     return L
 
@@ -285,6 +289,12 @@ class IEOperator:
 
     def set_fft_lines(self, lines: int):
         _check(lib().giem2g_set_fft_lines(self.handle, lines), "set_fft_lines")
+
+    def set_kernel_timing(self, on: bool):
+        _check(lib().giem2g_set_kernel_timing(self.handle, 1 if on else 0), "set_kernel_timing")
+
+    def last_contract_ms(self) -> float:
+        return float(lib().giem2g_last_contract_ms(self.handle))
 
     def check_device_error(self):
         _check(lib().giem2g_check_device_error(self.handle), "device error word")

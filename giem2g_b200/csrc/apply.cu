@@ -410,7 +410,11 @@ static int ie_apply_core(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t
     VecSet<CT<R>> vs{{d_in, nullptr}, {d_out, nullptr}, 1};
     dispatch_x<R>(true, op, vs, U1, st, gate);
     dispatch_y<R>(true, op, 1, U1, Uh, st, gate);
-    // contraction
+    // contraction (bracketed by events when kernel timing is on; never inside a stream capture)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    const bool timed = op->time_contract && op->evc0 &&
+                       cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone;
+    if (timed) cudaEventRecord(op->evc0, st);
     int rc_fast = G2_ERR_UNSUPPORTED;
     if (op->use_fast_contract) {
         if (sizeof(R) == 8)
@@ -427,6 +431,7 @@ static int ie_apply_core(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t
         const int threads = ((Z3 + 31) / 32) * 32;
         k_contract<R><<<(unsigned)op->units(), threads, sm, st>>>(G, Uh, Nx, Ny, Nz, gate);
     }
+    if (timed) cudaEventRecord(op->evc1, st);
     dispatch_y<R>(false, op, 1, U1, Uh, st, gate);
     dispatch_x<R>(false, op, vs, U1, st, gate);
     g2_count_launches(5);

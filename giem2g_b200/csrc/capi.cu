@@ -136,6 +136,8 @@ void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data
     }
     cudaEventCreate(&op->ev0);
     cudaEventCreate(&op->ev1);
+    cudaEventCreate(&op->evc0);
+    cudaEventCreate(&op->evc1);
     {
         const char *gen = std::getenv("GIEM2G_GENERIC_CONTRACT");
         op->use_fast_contract = !(gen && gen[0] == '1');
@@ -383,6 +385,23 @@ int giem2g_set_contract_variant(void *ie, int precision, int variant)
     op->contract_variant[precision] = variant;
     op->config_gen++;
     return set_status(0);
+}
+
+int giem2g_set_kernel_timing(void *ie, int on)
+{
+    IeOp *op = resolve(ie);
+    if (!op) return fail(G2_ERR_STATE, "giem2g_set_kernel_timing: no operator");
+    op->time_contract = on != 0;
+    return set_status(0);
+}
+
+double giem2g_last_contract_ms(void *ie)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !op->time_contract || cudaEventSynchronize(op->evc1) != cudaSuccess) return -1.0;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, op->evc0, op->evc1) != cudaSuccess) return -1.0;
+    return ms;
 }
 
 int giem2g_set_fft_lines(void *ie, int lines)
@@ -662,6 +681,8 @@ void giem2g_delete_ie_operator(void *ie)
         if (p) cudaFree(p);
     if (op->ev0) cudaEventDestroy(op->ev0);
     if (op->ev1) cudaEventDestroy(op->ev1);
+    if (op->evc0) cudaEventDestroy(op->evc0);
+    if (op->evc1) cudaEventDestroy(op->evc1);
     if (op->stream) cudaStreamDestroy(op->stream);
     if (g_last_op == op) g_last_op = nullptr;
     delete op;

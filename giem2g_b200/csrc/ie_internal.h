@@ -48,6 +48,9 @@ struct IeOp {
     double2 *d_vin = nullptr, *d_vout = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // events around the contraction launch of eager device applies (giem2g_set_kernel_timing)
+    bool time_contract = false;
+    cudaEvent_t evc0 = nullptr, evc1 = nullptr;
     int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
     bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
     int contract_variant[3] = {0, 0, 0};  // tile-shape variant: FP64, complex64, paired complex64

@@ -114,6 +114,10 @@ int giem2g_contract_variants(void *ie, int precision);  /* precision 2: paired c
 int giem2g_set_contract_variant(void *ie, int precision, int variant);
 /* Lines per CTA of the FFT passes (4, 8, 16 or 32; default 32), also set by the autotuner. */
 int giem2g_set_fft_lines(void *ie, int lines);
+/* Kernel timing: with on != 0, every device apply outside a stream capture records CUDA events around
+ * its contraction launch; giem2g_last_contract_ms returns the last one (ms, -1 if none). */
+int giem2g_set_kernel_timing(void *ie, int on);
+double giem2g_last_contract_ms(void *ie);
 /* CUDA stream the operator's kernels run on (cudaStream_t). */
 void *giem2g_get_stream(void *ie);
 /* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */
