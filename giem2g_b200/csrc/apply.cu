@@ -67,18 +67,20 @@ __global__ void __launch_bounds__(kThreads) k_fx(const VecSet<CT<R>> vs, const C
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw = reinterpret_cast<C *>(smem_raw);
     C *sm = tw + L;
+    // indices fit 32 bits: every buffer holds fewer than 2^31 elements for 2Nx, 2Ny <= 1024
     const int Z3 = 3 * Nz, ZL = vs.nv * Z3, zc0 = blockIdx.x * NL, y = blockIdx.y;
     const int nl = min(NL, ZL - zc0);
-    const size_t plane = (size_t)Nx * Ny;
+    const int plane = Nx * Ny, row = y * Nx;
     load_tw(tw, twg, L);
     __syncthreads();
     auto load = [&](int t, int x) -> C {
         const int zc = zc0 + t, v = zc >= Z3 ? 1 : 0, lzc = zc - v * Z3, z = lzc % Nz;
-        return cmul(vs.in[v][(size_t)lzc * plane + (size_t)y * Nx + x], gsig[(size_t)z * plane + (size_t)y * Nx + x]);
+        const C *in = v ? vs.in[1] : vs.in[0];  // select, not index: keeps the parameters out of local memory
+        return cmul(in[lzc * plane + row + x], gsig[z * plane + row + x]);
     };
-    auto store = [&](int t, int kx, C v) { U1[((size_t)kx * Ny + y) * ZL + zc0 + t] = v; };
+    auto store = [&](int t, int kx, C v) { U1[(kx * Ny + y) * ZL + zc0 + t] = v; };
     auto off = [&](int t, int n1, int k2) { return n1 + N1 * k2 + (L + 1) * t; };
-    fft4step<C, N1, N2, false, true, false, false, true>(sm, nl, tw, load, store, off);
+    fft4step<C, N1, N2, false, true, false, false, true>(sm, nl, ilog2(NL), tw, load, store, off);
 }
 
 // k_fy: zero-pad to 2Ny, forward y-FFT of one kx column, scatter to (q, r, slot).
@@ -109,14 +111,16 @@ __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, C
     }
     load_tw(tw, twg, L);
     __syncthreads();
-    auto load = [&](int t, int yy) -> C { return U1[((size_t)kx * Ny + yy) * Z3 + zc0 + t]; };
+    const C *col = U1 + kx * Ny * Z3 + zc0;
+    C *dst = Uh + q * Ny * 4 * Z3 + sx * 2 * Z3 + zc0;
+    auto load = [&](int t, int yy) -> C { return col[yy * Z3 + t]; };
     auto store = [&](int t, int ky, C v) {
         int r, sy;
         ky_to_slot(ky, Ny, r, sy);
-        Uh[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t] = v;
+        dst[(r * 4 + sy) * Z3 + t] = v;
     };
     auto off = [&](int t, int n1, int k2) { return t + NL * (n1 + N1 * k2); };
-    fft4step<C, N1, N2, false, true, false, true, true>(sm, nl, tw, load, store, off);
+    fft4step<C, N1, N2, false, true, false, true, true>(sm, nl, ilog2(NL), tw, load, store, off);
 }
 
 // k_by: inverse y-FFT of one kx column, crop y < Ny.  Distributed_FFT.F90:455-476, 696-788
@@ -138,14 +142,16 @@ __global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, C
     kx_to_slot(kx, Nx, q, sx);
     load_tw(tw, twg, L);
     __syncthreads();
+    const C *src = Uh + q * Ny * 4 * Z3 + sx * 2 * Z3 + zc0;
+    C *col = U1 + kx * Ny * Z3 + zc0;
     auto load = [&](int t, int ky) -> C {
         int r, sy;
         ky_to_slot(ky, Ny, r, sy);
-        return Uh[(((size_t)q * Ny + r) * 4 + sx * 2 + sy) * Z3 + zc0 + t];
+        return src[(r * 4 + sy) * Z3 + t];
     };
-    auto store = [&](int t, int yy, C v) { U1[((size_t)kx * Ny + yy) * Z3 + zc0 + t] = v; };
+    auto store = [&](int t, int yy, C v) { col[yy * Z3 + t] = v; };
     auto off = [&](int t, int n1, int k2) { return t + NL * (n1 + N1 * k2); };
-    fft4step<C, N1, N2, true, false, true, true, true>(sm, nl, tw, load, store, off);
+    fft4step<C, N1, N2, true, false, true, true, true>(sm, nl, ilog2(NL), tw, load, store, off);
 }
 
 // k_bx: inverse x-FFT, crop x < Nx, post-combine y = s*(a*x - w/(dz*4NxNy)).
@@ -164,25 +170,27 @@ __global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, c
     C *sm = tw + L;
     const int Z3 = 3 * Nz, ZL = vs.nv * Z3, zc0 = blockIdx.x * NL, y = blockIdx.y;
     const int nl = min(NL, ZL - zc0);
-    const size_t plane = (size_t)Nx * Ny;
+    const int plane = Nx * Ny, row = y * Nx;
     load_tw(tw, twg, L);
     __syncthreads();
     auto load = [&](int t, int kx) -> C {
-        return kx == Nx ? czero<C>() : U1[((size_t)kx * Ny + y) * ZL + zc0 + t];
+        return kx == Nx ? czero<C>() : U1[(kx * Ny + y) * ZL + zc0 + t];
     };
     auto store = [&](int t, int x, C w) {
         const int zc = zc0 + t, v = zc >= Z3 ? 1 : 0, lzc = zc - v * Z3, z = lzc % Nz;
-        const size_t cell = (size_t)z * plane + (size_t)y * Nx + x;
-        const size_t idx = (size_t)lzc * plane + (size_t)y * Nx + x;
-        const C d1 = cmul(vs.in[v][idx], asig[cell]);
+        const int cell = z * plane + row + x;
+        const int idx = lzc * plane + row + x;
+        const C *in = v ? vs.in[1] : vs.in[0];
+        C *out = v ? vs.out[1] : vs.out[0];
+        const C d1 = cmul(in[idx], asig[cell]);
         const R sq = post[z], inv = post[Nz + z];
         C o;
         o.x = (d1.x - w.x * inv) * sq;
         o.y = (d1.y - w.y * inv) * sq;
-        vs.out[v][idx] = o;
+        out[idx] = o;
     };
     auto off = [&](int t, int n1, int k2) { return t * (L + 1) + k2 + N2 * n1; };
-    fft4step<C, N1, N2, true, false, true, true, false>(sm, nl, tw, load, store, off);
+    fft4step<C, N1, N2, true, false, true, true, false>(sm, nl, ilog2(NL), tw, load, store, off);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -56,21 +56,25 @@ G2_D void reg_dft_dif(C (&a)[N], const C *tw, int Lstride)
     }
 }
 
-// One CTA transforms `nl` lines.  Functors:
+// One CTA transforms `nl` lines (nl <= 2^lg_nl, the CTA's line block).  Functors:
 //   load(line, idx) -> C            (step 1 input)
 //   store(line, idx, C)             (step 2 output)
 //   off(line, n1, k2) -> int        (shared-memory slot of the intermediate)
-// LF1/LF2: item ordering (true: line index fastest across threads; false: n1 / k2 fastest).
+// LF1/LF2: item ordering (true: line index fastest across threads; false: n1 / k2 fastest).  Items are
+// split with shifts and masks of the power-of-two line block; lines >= nl (a partial last block) are
+// skipped.
 template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
           class StoreF, class OffF>
-G2_D void fft4step(C *sm, int nl, const C *tw, LoadF load, StoreF store, OffF off)
+G2_D void fft4step(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF store, OffF off)
 {
     constexpr int L = N1 * N2;
-    const int n_items1 = nl * N1;
+    const int nlb = 1 << lg_nl;
+    const int n_items1 = (LF1 ? nlb : nl) * N1;
     for (int it = threadIdx.x; it < n_items1; it += blockDim.x) {
         int line, n1;
-        if (LF1) { line = it % nl; n1 = it / nl; }
+        if (LF1) { line = it & (nlb - 1); n1 = it >> lg_nl; }
         else { n1 = it % N1; line = it / N1; }
+        if (LF1 && line >= nl) continue;
         C a[N2];
 #pragma unroll
         for (int n2 = 0; n2 < N2; n2++) {
@@ -86,11 +90,12 @@ G2_D void fft4step(C *sm, int nl, const C *tw, LoadF load, StoreF store, OffF of
         }
     }
     __syncthreads();
-    const int n_items2 = nl * N2;
+    const int n_items2 = (LF2 ? nlb : nl) * N2;
     for (int it = threadIdx.x; it < n_items2; it += blockDim.x) {
         int line, k2;
-        if (LF2) { line = it % nl; k2 = it / nl; }
+        if (LF2) { line = it & (nlb - 1); k2 = it >> lg_nl; }
         else { k2 = it % N2; line = it / N2; }
+        if (LF2 && line >= nl) continue;
         C a[N1];
 #pragma unroll
         for (int n1 = 0; n1 < N1; n1++) a[n1] = sm[off(line, n1, k2)];
