@@ -154,7 +154,8 @@ int giem2g_solve_device(void *ie, const void *d_E_bkg, void *d_Esol, const void 
                         GIEM2G_RESULT *info);
 /* Outer Arnoldi misfit after each outer iteration of the last solve; returns the count copied. */
 int giem2g_get_misfit_history(void *ie, double *out, int max_len);
-/* Outer right preconditioner hook (no counterpart in the reference; the learned preconditioner).
+/* Outer right preconditioner hook: the slot that SET_RIGHT_PRECONDTIONER (seq_fgmres.F90:92-102) fills
+ * with the inner GMRES in the reference, here open to the learned preconditioner.
  * fn(user, d_v, d_z, n, stream) receives V_j (complex128, n elements, device) and writes its guess of
  * A^-1 V_j to d_z (complex128, device) on `stream`, returning 0 (nonzero: the hook is dropped for the
  * rest of the solve).  mode 1: the guess starts the inner GMRES cycle (x0 = guess instead of x0 = V_j);
