@@ -1,0 +1,105 @@
+"""Driver for the IE solve path with the reference's input and output files.
+
+    python -m giem2g_b200.driver input.json [--precision 0|1] [--outdir DIR]
+
+Restates the solve part of the reference's main program (giem2g.F90:336-373, 430-470): read the JSON
+input (background, anomaly grid and conductivity file, frequencies, FGMRES settings), then for every
+frequency in order build the Green's tensor on the GPU, transform it, set the anomaly conductivity and
+solve the plane-wave problem for EY, then EX.  The initial guess of each solve follows the reference:
+a solution file of the same frequency and polarisation if one exists in the output directory, else
+nothing for the first frequency, else the previous frequency's solution of that polarisation.  With
+"Save Solution" true every solution is written as SOL_P{Y,X}_F<freq>.bin.  Receiver fields
+("Recalculate Fields") are not part of this library and are reported as skipped.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from .solution_io import EX, EY, load_input, load_solution, read_sigma_text, save_solution, solution_name
+
+
+def model_from_input(inp: dict, base_dir: str):
+    """(IEModel at the first frequency, conductivity [Ny, Nx, Nz], frequencies, FGMRES settings)."""
+    from .synthetic import IEModel
+    bkg, an = inp["Background"], inp["Anomaly"]
+    sigma = np.asarray(bkg["Conductivity"], dtype=np.float64)
+    thick = np.asarray(bkg.get("Thickness", []), dtype=np.float64)[: len(sigma) - 1]
+    Nx, Ny, Nz = int(an["Nx"]), int(an["Ny"]), int(an["Nz"])
+    z = np.asarray(an["zborders"], dtype=np.float64)[: Nz + 1]
+    freqs = [float(f) for f in inp["Frequencies"]]
+    m = IEModel(Nx, Ny, Nz, float(an["dx"]), float(an["dy"]), z, sigma, thick, freqs[0])
+    cpath = an["Conductivity"]
+    if not os.path.isabs(cpath) and not os.path.exists(cpath):
+        cpath = os.path.join(base_dir, cpath)
+    sig = read_sigma_text(cpath, Nx, Ny, Nz)
+    fg = inp.get("FGMRES", {})
+    ctl = {"outer_buf": int(fg.get("OuterBufferSize", 30)), "inner_buf": int(fg.get("InnerBufferSize", 10)),
+           "max_restart": int(fg.get("MaxRestart", 100)), "tol": float(fg.get("Tolerance", 1e-8))}
+    return m, sig, freqs, ctl
+
+
+def run(input_path: str, precision: int = 0, outdir: str | None = None, log=print) -> dict:
+    from . import IEOperator
+    from .sources import plane_wave_integral
+    inp = load_input(input_path)
+    base = os.path.dirname(os.path.abspath(input_path))
+    outdir = outdir or os.getcwd()
+    m0, sig, freqs, ctl = model_from_input(inp, base)
+    solve = bool(inp.get("Solve Equation", True))
+    save = bool(inp.get("Save Solution", False))
+    out = {"grid": [m0.Nx, m0.Ny, m0.Nz], "frequencies": freqs, "precision": precision, "solves": []}
+    if inp.get("Recalculate Fields", False):
+        out["recalculate_fields"] = "skipped: receiver fields are outside this library"
+    if not solve:
+        return out
+    op = IEOperator.from_model(m0)
+    prev = {EY: None, EX: None}
+    try:
+        for i, f in enumerate(freqs):
+            m = m0.with_freq(f)
+            t0 = time.perf_counter()
+            op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+            op.calc_fft_of_ie_kernel()
+            op.set_anomaly_sigma(sig, f)
+            t_setup = time.perf_counter() - t0
+            for pol in (EY, EX):
+                name = os.path.join(outdir, solution_name(pol, f))
+                guess = load_solution(name, m.Nx, m.Ny, m.Nz)
+                source = "file" if guess is not None else ("previous frequency" if i > 0 else "none")
+                if guess is None and i > 0:
+                    guess = prev[pol]
+                E_bkg = plane_wave_integral(m, pol)
+                E, info = op.solve_equation(E_bkg, E0=guess, tol=ctl["tol"], max_restart=ctl["max_restart"],
+                                            outer_buf=ctl["outer_buf"], inner_buf=ctl["inner_buf"],
+                                            precision=precision)
+                prev[pol] = E
+                if save:
+                    save_solution(name, E)
+                row = {"freq": f, "pol": "EY" if pol == EY else "EX", "guess": source,
+                       "iterations": info.iterations, "stat": info.stat, "true_rel_residual": info.be,
+                       "device_ms": info.device_ms, "setup_s": t_setup}
+                out["solves"].append(row)
+                if log:
+                    log(json.dumps(row))
+    finally:
+        op.delete()
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="IE solves of a GIEM2G input file on one GPU")
+    ap.add_argument("input")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1], help="0: FP64, 1: mixed")
+    ap.add_argument("--outdir", default=None, help="directory of the SOL_*.bin files (default: cwd)")
+    args = ap.parse_args(argv)
+    res = run(args.input, args.precision, args.outdir)
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

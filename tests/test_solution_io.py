@@ -1,0 +1,56 @@
+"""File formats of the reference's driver (solution files, conductivity text, input JSON) on the CPU."""
+import json
+import os
+
+import numpy as np
+
+from giem2g_b200.solution_io import (EX, EY, freq_string, load_input, load_solution, read_sigma_text,
+                                     save_solution, solution_name)
+
+
+def test_frequency_tag_matches_f22_10_with_leading_zeros():
+    assert freq_string(0.1) == "00000000000.1000000000"
+    assert freq_string(100.0) == "00000000100.0000000000"
+    assert freq_string(0.001) == "00000000000.0010000000"
+    assert len(freq_string(3.7275937203149416)) == 22
+    assert solution_name(EY, 1.0) == "SOL_PY_F00000000001.0000000000.bin"
+    assert solution_name(EX, 1.0) == "SOL_PX_F00000000001.0000000000.bin"
+
+
+def test_solution_file_order_is_z_c_x_y(tmp_path):
+    Nx, Ny, Nz = 4, 3, 2
+    rng = np.random.default_rng(1)
+    E = rng.standard_normal((3, Nz, Ny, Nx)) + 1j * rng.standard_normal((3, Nz, Ny, Nx))
+    p = tmp_path / "s.bin"
+    save_solution(str(p), E)
+    raw = np.fromfile(p, dtype="<c16")
+    assert raw.size == E.size
+    # element (z, c, x, y) of the file sits at z + Nz*(c + 3*(x + Nx*y))
+    for (z, c, x, y) in [(0, 0, 0, 0), (1, 2, 3, 2), (0, 1, 2, 1), (1, 0, 1, 0)]:
+        assert raw[z + Nz * (c + 3 * (x + Nx * y))] == E[c, z, y, x]
+    back = load_solution(str(p), Nx, Ny, Nz)
+    assert np.array_equal(back, E)
+    assert load_solution(str(tmp_path / "missing.bin"), Nx, Ny, Nz) is None
+
+
+def test_sigma_text_list_directed(tmp_path):
+    Nx, Ny, Nz = 3, 2, 2
+    vals = np.arange(1, Nx * Ny * Nz + 1, dtype=float) * 1e-3
+    p = tmp_path / "sig.dat"
+    # blanks, commas, new lines, a repeat count and D exponents, as a list-directed READ accepts
+    toks = [f"{v:.3E}".replace("E", "D") for v in vals[:6]] + ["2*7.000E-03"]
+    body = " ".join(toks[:3]) + ",\n" + ", ".join(toks[3:]) + "\n" + "\n".join(f"{v}" for v in vals[8:])
+    p.write_text(body)
+    vals2 = vals.copy()
+    vals2[6:8] = 7e-3
+    s = read_sigma_text(str(p), Nx, Ny, Nz)
+    assert s.shape == (Ny, Nx, Nz)
+    assert np.allclose(s.ravel(), vals2)
+    assert s[1, 2, 0] == vals2[0 + Nz * (2 + Nx * 1)]  # siga(z, x, y) with z fastest
+
+
+def test_input_json_with_trailing_commas(tmp_path):
+    p = tmp_path / "in.json"
+    p.write_text('{"Frequencies": [0.1, 1.0,], "FGMRES": {"Tolerance": 1e-8,}, "Recievers": [{"depth": 0},],}')
+    d = load_input(str(p))
+    assert d["Frequencies"] == [0.1, 1.0] and d["FGMRES"]["Tolerance"] == 1e-8
