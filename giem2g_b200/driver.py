@@ -43,7 +43,7 @@ def model_from_input(inp: dict, base_dir: str):
     return m, sig, freqs, ctl
 
 
-def run(input_path: str, precision: int = 0, outdir: str | None = None, log=print) -> dict:
+def run(input_path: str, precision: int = 0, outdir: str | None = None, log=print, warm_start: bool = True) -> dict:
     from . import IEOperator
     from .sources import plane_wave_integral
     inp = load_input(input_path)
@@ -71,8 +71,10 @@ def run(input_path: str, precision: int = 0, outdir: str | None = None, log=prin
                 name = os.path.join(outdir, solution_name(pol, f))
                 guess = load_solution(name, m.Nx, m.Ny, m.Nz)
                 source = "file" if guess is not None else ("previous frequency" if i > 0 else "none")
-                if guess is None and i > 0:
+                if guess is None and i > 0 and warm_start:
                     guess = prev[pol]
+                elif guess is None:
+                    source = "none"
                 E_bkg = plane_wave_integral(m, pol)
                 E, info = op.solve_equation(E_bkg, E0=guess, tol=ctl["tol"], max_restart=ctl["max_restart"],
                                             outer_buf=ctl["outer_buf"], inner_buf=ctl["inner_buf"],
@@ -96,8 +98,9 @@ def main(argv=None):
     ap.add_argument("input")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1], help="0: FP64, 1: mixed")
     ap.add_argument("--outdir", default=None, help="directory of the SOL_*.bin files (default: cwd)")
+    ap.add_argument("--cold", action="store_true", help="no previous-frequency guess (for comparison)")
     args = ap.parse_args(argv)
-    res = run(args.input, args.precision, args.outdir)
+    res = run(args.input, args.precision, args.outdir, warm_start=not args.cold)
     print(json.dumps(res))
 
 
