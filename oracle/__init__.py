@@ -48,6 +48,12 @@ def lib():
         L.orc_vbt_weights.argtypes = [dp, dp, dp, dp, dp, vp, vp]
         L.orc_background_cells.argtypes = [vp, vp, vp]
         L.orc_layer_numbers.argtypes = [vp, vp]
+        L.orc_prepare_receivers.argtypes = [vp, ip, vp, vp, vp]
+        L.orc_vbt_weights_single.argtypes = [dp, dp, dp, dp, dp, vp, vp]
+        L.orc_rc_tensor.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, ip]
+        L.orc_rc_apply_direct.argtypes = [ip, ip, ip, ip, vp, vp, vp, vp, vp, vp, ip]
+        L.orc_rc_apply_fft.argtypes = [ip, ip, ip, ip, vp, vp, vp, vp, vp, vp, ip]
+        L.orc_plane_wave_points.argtypes = [vp, ip, ip, vp, vp]
         L.orc_eps0.restype = dp
         L.orc_mu0.restype = dp
         _lib = L
@@ -165,6 +171,71 @@ def vbt_weights(x, y, hx, hy, rmin):
     lms = np.zeros(501, np.float64)
     lib().orc_vbt_weights(x, y, hx, hy, rmin, _p(WT), _p(lms))
     return WT, lms
+
+
+def vbt_weights_single(x, y, hx, hy, rmin):
+    """VBTransformWeightsAllSingleInt (VolumeBesselTransforms.F90:198-229): WT[501, 6], lms[501]."""
+    WT = np.zeros((501, 6), np.float64)
+    lms = np.zeros(501, np.float64)
+    lib().orc_vbt_weights_single(x, y, hx, hy, rmin, _p(WT), _p(lms))
+    return WT, lms
+
+
+@dataclass
+class Receivers:
+    """Receivers after PrepareRecvs (data_types_module.F90:124-152)."""
+    zrecv: np.ndarray
+    x_shift: np.ndarray
+    y_shift: np.ndarray
+    recv_layer: np.ndarray
+    anom_cell: np.ndarray
+
+    @property
+    def Nr(self):
+        return len(self.zrecv)
+
+
+def prepare_receivers(m, zrecv, x_shift=None, y_shift=None) -> Receivers:
+    z = _f64(np.array(zrecv, dtype=np.float64))
+    Nr = len(z)
+    xs = _f64(np.zeros(Nr) if x_shift is None else x_shift)
+    ys = _f64(np.zeros(Nr) if y_shift is None else y_shift)
+    rl = np.zeros(Nr, np.int32)
+    ac = np.zeros(Nr, np.int32)
+    s, keep = _model_struct(m)
+    lib().orc_prepare_receivers(ctypes.byref(s), Nr, _p(z), _p(rl), _p(ac))
+    return Receivers(z, xs, ys, rl, ac)
+
+
+def rc_tensor(m, rv: Receivers, nthreads: int = 0):
+    """Spatial receiver tensor [2Ny, 2Nx, 15, Nr, Nz] (calc_rc_tensor_module.F90:38-229)."""
+    G = np.zeros((2 * m.Ny, 2 * m.Nx, 15, rv.Nr, m.Nz), np.complex128)
+    s, keep = _model_struct(m)
+    lib().orc_rc_tensor(ctypes.byref(s), rv.Nr, _p(rv.zrecv), _p(rv.x_shift), _p(rv.y_shift), _p(rv.recv_layer),
+                        _p(rv.anom_cell), _p(G), nthreads)
+    return G
+
+
+def rc_apply(Nx, Ny, Nz, G, csiga, csigb, E, direct: bool = False, nthreads: int = 0):
+    """ReCalculation (Continuation_Function_Module.F90:198-239): anomalous fields at the receivers,
+    Ea, Ha [Ny, Nx, 3, Nr], from the anomaly field E [3, Nz, Ny, Nx].  direct=True sums the lags
+    directly instead of going through the FFT."""
+    G, csiga, csigb, E = _c128(G), _c128(csiga), _c128(csigb), _c128(E)
+    Nr = G.shape[3]
+    Ea = np.zeros((Ny, Nx, 3, Nr), np.complex128)
+    Ha = np.zeros_like(Ea)
+    fn = lib().orc_rc_apply_direct if direct else lib().orc_rc_apply_fft
+    fn(Nx, Ny, Nz, Nr, _p(G), _p(csiga), _p(csigb), _p(E), _p(Ea), _p(Ha), nthreads)
+    return Ea, Ha
+
+
+def plane_wave_points(m, pol: int, zrecv):
+    """PlaneWave (sources_module.F90:26-66): F[Nr, 6] = Ex Ey Ez Hx Hy Hz at the receiver depths."""
+    z = _f64(np.array(zrecv, dtype=np.float64))
+    F = np.zeros((len(z), 6), np.complex128)
+    s, keep = _model_struct(m)
+    lib().orc_plane_wave_points(ctypes.byref(s), pol, len(z), _p(z), _p(F))
+    return F
 
 
 def eps0() -> float:

@@ -324,16 +324,17 @@ static void vbt_out_int4(const vbt_edt *e, int i, double R[6])
     R[5] = R[5] / e->explt2[i];
 }
 
-/* :264-288 CalcWeights22 (non-Ooura branch). WT[k][6] for k = NFIRST..NLAST */
-static void vbt_calc_weights22(const vbt_tables *t, const vbt_edt *e, double *WT)
+/* :264-288 CalcWeights22 (non-Ooura branch) with the output function `outf`. WT[k][6] for k = NFIRST..NLAST */
+typedef void (*vbt_outfunc)(const vbt_edt *e, int i, double R[6]);
+static void vbt_calc_weights22_f(const vbt_tables *t, const vbt_edt *e, double *WT, vbt_outfunc outf)
 {
     double complex *g = (double complex *)malloc(sizeof(double complex) * VBT_N * 6);
     double complex *h = (double complex *)malloc(sizeof(double complex) * VBT_N * 6);
     double R[6];
     for (int i = 0; i < VBT_N; i += 2) {
-        vbt_out_int4(e, i, R);
+        outf(e, i, R);
         for (int c = 0; c < 6; c++) g[(size_t)t->inds[i] * 6 + c] = R[c];
-        vbt_out_int4(e, i + 1, R);
+        outf(e, i + 1, R);
         for (int c = 0; c < 6; c++) g[(size_t)t->inds[i + 1] * 6 + c] = -R[c];
     }
     vbt_fft(g, 6, t->w_fwd);
@@ -352,6 +353,11 @@ static void vbt_calc_weights22(const vbt_tables *t, const vbt_edt *e, double *WT
         for (int c = 0; c < 6; c++) WT[(size_t)(k - NFIRST) * 6 + c] = creal(h[(size_t)k * 6 + c]);
     free(g);
     free(h);
+}
+
+static void vbt_calc_weights22(const vbt_tables *t, const vbt_edt *e, double *WT)
+{
+    vbt_calc_weights22_f(t, e, WT, vbt_out_int4);
 }
 
 /* :159-197 VBTransformWeightsAllDoubleInt */
@@ -1514,5 +1520,553 @@ int orc_solve(int Nx, int Ny, int Nz, const double complex *symm_hat, const doub
     gm_free(&inner);
     free(rhs);
     free(guess);
+    return 0;
+}
+
+/* ========================================================================= */
+/* Receiver continuation (fields at receivers from the anomaly's currents)   */
+/* Continuation_Function_Module.F90, calc_rc_tensor_module.F90,              */
+/* rc_kernel_hankel_module.F90, VolumeBesselTransforms.F90 (single integral) */
+/* ========================================================================= */
+
+/* data_types_module.F90:124-152 PrepareRecvs: receiver layer and the number of anomaly cells above it;
+ * a receiver strictly inside a cell is moved to the cell's top border. */
+int orc_prepare_receivers(const orc_model *m, int Nr, double *zrecv, int *recv_layer, int *anom_cell)
+{
+    double depth[m->Nl + 1];
+    make_depth(m, depth);
+    int Nz = m->Nz;
+    for (int i = 0; i < Nr; i++) {
+        double zr = zrecv[i];
+        int l = orc_get_layer(zr, m->Nl, depth);
+        recv_layer[i] = l > 1 ? l : 1;
+        if (zr <= m->z[0]) {
+            anom_cell[i] = 0;
+        } else if (zr >= m->z[Nz]) {
+            anom_cell[i] = Nz + 1;
+        } else {
+            for (int iz = 1; iz <= Nz; iz++) {
+                if (fabs(zr / m->z[iz] - 1.0) < 1e-7) {
+                    anom_cell[i] = iz;
+                    break;
+                } else if (zr > m->z[iz - 1] && zr < m->z[iz]) {
+                    zrecv[i] = m->z[iz - 1];
+                    anom_cell[i] = iz - 1;
+                    break;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+/* VolumeBesselTransforms.F90:342-371 PrepareExps2 */
+static void vbt_prepare_exps2(double phi, double alpha, double beta, vbt_edt *e)
+{
+    double cphi = cos(phi), sphi = sin(phi);
+    for (int i = 0; i < VBT_N; i++) {
+        double x1 = e->explt[i] * cphi * 0.5;
+        double y1 = e->explt[i] * sphi * 0.5;
+        double dxv = alpha * e->explt[i] * 0.5;
+        double dyv = beta * e->explt[i] * 0.5;
+        double x[2] = {x1, x1 + dxv}, y[2] = {y1, y1 + dyv};
+        for (int k = 0; k < 2; k++) {
+            double x2 = x[k] * x[k];
+            e->xy_exp2[0][i][k] = exp(-x2);
+            e->xy_erf[0][i][k] = erf(x[k]);
+            e->xy[0][i][k] = x[k];
+            e->xy2[0][i][k] = x2;
+            double y2 = y[k] * y[k];
+            e->xy_exp2[1][i][k] = exp(-y2);
+            e->xy_erf[1][i][k] = erf(y[k]);
+            e->xy[1][i][k] = y[k];
+            e->xy2[1][i][k] = y2;
+        }
+    }
+}
+
+static void vbt_single_int_d0(const vbt_edt *e, int i, int j, double R[3]) /* :553-567 */
+{
+    const double *x = e->xy[j][i], *x2 = e->xy2[j][i], *ex = e->xy_exp2[j][i], *er = e->xy_erf[j][i];
+    double f[2];
+    for (int k = 0; k < 2; k++) f[k] = er[k] * SPI_D;
+    double a = f[1] - f[0];
+    R[0] = a * 0.5;
+    for (int k = 0; k < 2; k++) f[k] = x[k] * ex[k];
+    double b = f[1] - f[0];
+    R[1] = a - 2.0 * b;
+    for (int k = 0; k < 2; k++) f[k] = f[k] * x2[k];
+    double c = f[1] - f[0];
+    R[2] = 6.0 * a - 12.0 * b - 8.0 * c;
+}
+static void vbt_single_int_d1(const vbt_edt *e, int i, int j, double R[3]) /* :569-585 */
+{
+    const double *x2 = e->xy2[j][i], *ex = e->xy_exp2[j][i];
+    double f[2];
+    for (int k = 0; k < 2; k++) f[k] = ex[k];
+    R[0] = f[1] - f[0];
+    for (int k = 0; k < 2; k++) f[k] = f[k] * x2[k];
+    R[1] = f[1] - f[0];
+    for (int k = 0; k < 2; k++) f[k] = f[k] * x2[k];
+    R[2] = f[1] - f[0];
+    R[0] = R[0] / 2.0;
+    R[1] = R[1] * 2.0;
+    R[2] = R[2] * 8.0;
+}
+static void vbt_single_int_d2(const vbt_edt *e, int i, int j, double R[3]) /* :587-603 */
+{
+    const double *x = e->xy[j][i], *x2 = e->xy2[j][i], *ex = e->xy_exp2[j][i];
+    double f[2];
+    for (int k = 0; k < 2; k++) f[k] = x[k] * ex[k];
+    double a = f[1] - f[0];
+    R[0] = -a * 0.5;
+    for (int k = 0; k < 2; k++) f[k] = f[k] * x2[k];
+    double b = f[1] - f[0];
+    R[1] = 2.0 * (a - b);
+    for (int k = 0; k < 2; k++) f[k] = f[k] * x2[k];
+    double c = f[1] - f[0];
+    R[2] = 16.0 * b - 8.0 * c;
+}
+
+/* :407-434 outfunc_int2_all */
+static void vbt_out_int2(const vbt_edt *e, int i, double R[6])
+{
+    double fx[3][3], fy[3][3];
+    vbt_single_int_d0(e, i, 0, fx[0]);
+    vbt_single_int_d1(e, i, 0, fx[1]);
+    vbt_single_int_d2(e, i, 0, fx[2]);
+    vbt_single_int_d0(e, i, 1, fy[0]);
+    vbt_single_int_d1(e, i, 1, fy[1]);
+    vbt_single_int_d2(e, i, 1, fy[2]);
+#define FX(k, D) fx[D][(k)-1]
+#define FY(k, D) fy[D][(k)-1]
+    R[0] = FX(3, 0) * FY(1, 0) + FX(1, 0) * FY(3, 0) + 2.0 * FX(2, 0) * FY(2, 0);
+    R[1] = FX(3, 2) * FY(1, 0) + FX(1, 2) * FY(3, 0) + 2.0 * FX(2, 2) * FY(2, 0);
+    R[2] = FX(3, 1) * FY(1, 1) + FX(1, 1) * FY(3, 1) + 2.0 * FX(2, 1) * FY(2, 1);
+    R[3] = FX(3, 1) * FY(1, 0) + FX(1, 1) * FY(3, 0) + 2.0 * FX(2, 1) * FY(2, 0);
+    R[4] = FX(3, 0) * FY(1, 2) + FX(1, 0) * FY(3, 2) + 2.0 * FX(2, 0) * FY(2, 2);
+    R[5] = FX(3, 0) * FY(1, 1) + FX(1, 0) * FY(3, 1) + 2.0 * FX(2, 0) * FY(2, 1);
+#undef FX
+#undef FY
+    R[0] = R[0] / e->explt[i];
+    R[1] = R[1] * e->explt[i];
+    R[2] = R[2] * e->explt[i];
+    R[4] = R[4] * e->explt[i];
+}
+
+/* :198-229 VBTransformWeightsAllSingleInt: WT[k][6] (columns in the routine's own order) */
+static void vbt_weights_single_int(const vbt_tables *t, double x, double y, double hx, double hy, double *WT)
+{
+    double rho = sqrt(x * x + y * y);
+    double alpha = hx / rho, beta = hy / rho, phi = atan2(y, x);
+    vbt_edt *e = (vbt_edt *)malloc(sizeof(vbt_edt));
+    vbt_calc_exp_lt(log(rho) - t->lambda_shift, e);
+    vbt_prepare_exps2(phi, alpha, beta, e);
+    vbt_calc_weights22_f(t, e, WT, vbt_out_int2);
+    for (int k = 0; k < NLAM; k++) {
+        WT[k * 6 + 0] = WT[k * 6 + 0] * rho;
+        WT[k * 6 + 1] = WT[k * 6 + 1] / rho;
+        WT[k * 6 + 2] = WT[k * 6 + 2] / rho;
+        WT[k * 6 + 4] = WT[k * 6 + 4] / rho;
+    }
+    free(e);
+}
+
+int orc_vbt_weights_single(double x, double y, double hx, double hy, double rmin, double *WT, double *lms)
+{
+    vbt_tables *t = (vbt_tables *)malloc(sizeof(vbt_tables));
+    vbt_init(rmin, t);
+    vbt_weights_single_int(t, x, y, hx, hy, WT);
+    if (lms) memcpy(lms, t->lms, sizeof(double) * NLAM);
+    free(t);
+    return 0;
+}
+
+/* rc_kernel_hankel_module.F90:31-38 weight indices and :47-54 G indices (0-based here) */
+enum { RC_DXX = 0, RC_DXY = 1, RC_DYY = 2, RC_DX = 3, RC_DY = 4, RC_D0 = 5 };
+enum { RG1 = 0, RG3DZ, RG2DZ, RG2DZ0, RG2G2DZZ, RG3, RG1DZ, RG2 };
+/* const_module.F90:112-130 component slots; E: XX XY XZ YY YZ ZX ZY ZZ, H: XX XY XZ YX YZ ZX ZY */
+enum { REXX = 0, REXY, REXZ, REYY, REYZ, REZX, REZY, REZZ };
+enum { RHXX = 0, RHXY, RHXZ, RHYX, RHYZ, RHZX, RHZY };
+
+typedef struct {
+    double zrecv;
+    int recv_layer, anom_cell;
+} rc_recv_t;
+
+/* rc_kernel_hankel_module.F90:181-225 Calc_Recv_Part; w1, w2 are [Nz+1][2] */
+static void rc_recv_part(const bkg_t *b, const anom_t *an, double complex (*p)[2], double complex (*q)[2],
+                         const double complex *eta, const rc_recv_t *rv, double complex (*w1)[2],
+                         double complex (*w2)[2])
+{
+    int rl = rv->recv_layer, Nz = an->Nz;
+    double complex eta_r = eta[rl];
+    double complex eta_zr = eta_r * rv->zrecv;
+    double complex eta_dr = rl > 1 ? eta_r * b->depth[rl - 1] * 2.0 : 0.0;
+    int N = rv->anom_cell;
+    int N1 = N + 1 > 1 ? N + 1 : 1;
+    int N2 = N < Nz ? N : Nz;
+    for (int i = N1; i <= Nz; i++) {
+        int l = an->L[i];
+        double complex e1 = cexp(-an->z[i - 1] * eta[l] + eta_zr);
+        double complex e2 = cexp(-an->z[i - 1] * eta[l] - eta_zr + eta_dr);
+        w1[i][0] = (e2 * p[rl][0] + e1);
+        w1[i][1] = (-e2 * p[rl][0] + e1) * eta_r;
+        w2[i][0] = (e2 * p[rl][1] + e1);
+        w2[i][1] = (-e2 * p[rl][1] + e1) * eta_r;
+    }
+    if (rl < b->Nl) eta_dr = eta_r * b->depth[rl] * 2.0;
+    else eta_dr = 1.0 * 1.7976931348623157e308; /* HUGE(zrecv) */
+    for (int i = 1; i <= N2; i++) {
+        int l = an->L[i];
+        double complex e1 = cexp(an->z[i] * eta[l] - eta_zr);
+        double complex e2 = cexp(an->z[i] * eta[l] + eta_zr - eta_dr);
+        w1[i][0] = (e2 * q[rl][0] + e1);
+        w1[i][1] = (e2 * q[rl][0] - e1) * eta_r;
+        w2[i][0] = (e2 * q[rl][1] + e1);
+        w2[i][1] = (e2 * q[rl][1] - e1) * eta_r;
+    }
+}
+
+/* rc_kernel_hankel_module.F90:227-252 Calc_Ftb; Ftb is [Nz+1][3] */
+static void rc_ftb(const anom_t *an, const double complex *expz, const double complex *eta,
+                   double complex (*pq)[2], int N1, int N2, double complex (*Ftb)[3], double s)
+{
+    for (int i = N1; i <= N2; i++) {
+        int l = an->L[i];
+        double complex a = (1.0 - expz[i]);
+        double complex a1 = a / eta[l];
+        double complex e1[2], e2[2];
+        for (int k = 0; k < 2; k++) {
+            e1[k] = 1.0 + pq[i][k] * expz[i];
+            e2[k] = (1.0 - pq[i][k] * expz[i]) * s;
+        }
+        Ftb[i][0] = a1 * e1[0];
+        Ftb[i][1] = a1 * e1[1];
+        Ftb[i][2] = a * e2[1];
+    }
+}
+
+/* rc_kernel_hankel_module.F90:56-145 Calc_Integral_U with Calc_G_not_match (:147-179).
+ * GE1 [Nz+1][8], GH1 [Nz+1][7] accumulate over lambda. */
+static void rc_integral_u(const bkg_t *b, const anom_t *an, const rc_recv_t *rv, double lms, const double *W,
+                          double complex (*GE1)[8], double complex (*GH1)[7])
+{
+    int Nl = b->Nl, Nz = an->Nz;
+    double complex A[(Nl + 1) * (Nl + 1) * 2];
+    double complex p[Nl + 1][2], q[Nl + 1][2], eta[Nl + 1], Arr[Nl + 1][2];
+    double complex expz[Nz + 1], pez[Nz + 1][2], qez[Nz + 1][2], w1[Nz + 1][2], w2[Nz + 1][2], Ftb[Nz + 1][3];
+    double lm2 = lms * lms;
+    calc_apq(b, lms, Arr, p, q, eta, A);
+    for (int iz = 1; iz <= Nz; iz++) expz[iz] = cexp(-eta[an->L[iz]] * (an->z[iz] - an->z[iz - 1]));
+    rc_recv_part(b, an, p, q, eta, rv, w1, w2);
+    memset(Ftb, 0, sizeof(Ftb));
+    if (rv->anom_cell < 1) {
+        calc_qexpz(b, an, expz, eta, q, qez);
+        rc_ftb(an, expz, eta, qez, 1, Nz, Ftb, 1.0);
+    } else if (rv->anom_cell > Nz) {
+        calc_pexpz(b, an, expz, eta, p, pez);
+        rc_ftb(an, expz, eta, pez, 1, Nz, Ftb, -1.0);
+    } else {
+        int N = rv->anom_cell;
+        calc_pexpz(b, an, expz, eta, p, pez);
+        calc_qexpz(b, an, expz, eta, q, qez);
+        rc_ftb(an, expz, eta, pez, 1, N, Ftb, -1.0);
+        rc_ftb(an, expz, eta, qez, N + 1, Nz, Ftb, 1.0);
+    }
+    int rl = rv->recv_layer;
+    double complex csr = b->csigma[rl];
+#define AIX(i, j, k) A[(((size_t)(i) * (Nl + 1)) + (j)) * 2 + (k)]
+    for (int i = 1; i <= Nz; i++) {
+        int l = an->L[i];
+        double complex a1 = AIX(rl, l, 0), a2 = AIX(rl, l, 1);
+        double complex *f = Ftb[i];
+        double complex G[8];
+        G[RG1] = a1 * f[0] * w1[i][0];
+        G[RG3DZ] = (a2 * f[2] * w2[i][1]) / csr;
+        G[RG2DZ] = (a2 * f[1] * w2[i][1]) / csr;
+        G[RG2DZ0] = (a2 * f[2] * w2[i][0]) / csr;
+        G[RG2G2DZZ] = lm2 * (a2 * f[1] * w2[i][0]) / csr;
+        G[RG3] = (a2 * f[2] * w2[i][0] - a1 * f[0] * w1[i][1]);
+        G[RG1DZ] = a1 * f[0] * w1[i][1];
+        G[RG2] = a2 * f[1] * w2[i][0];
+        double complex G11 = G[RG1] * b->iwm;
+        GE1[i][REXX] = GE1[i][REXX] + G11 * W[RC_D0] + (G[RG3DZ] + G11) * W[RC_DXX];
+        GE1[i][REXY] = GE1[i][REXY] + (G[RG3DZ] + G11) * W[RC_DXY];
+        GE1[i][REXZ] = GE1[i][REXZ] + G[RG2DZ] * W[RC_DX];
+        GE1[i][REYY] = GE1[i][REYY] + G11 * W[RC_D0] + (G[RG3DZ] + G11) * W[RC_DYY];
+        GE1[i][REYZ] = GE1[i][REYZ] + G[RG2DZ] * W[RC_DY];
+        GE1[i][REZX] = GE1[i][REZX] + G[RG2DZ0] * W[RC_DX];
+        GE1[i][REZY] = GE1[i][REZY] + G[RG2DZ0] * W[RC_DY];
+        GE1[i][REZZ] = GE1[i][REZZ] + G[RG2G2DZZ] * W[RC_D0];
+        GH1[i][RHXX] = GH1[i][RHXX] + G[RG3] * W[RC_DXY];
+        GH1[i][RHXY] = GH1[i][RHXY] + G[RG3] * W[RC_DYY] - G[RG1DZ] * W[RC_D0];
+        GH1[i][RHXZ] = GH1[i][RHXZ] + G[RG2] * W[RC_DY];
+        GH1[i][RHYX] = GH1[i][RHYX] + G[RG1DZ] * W[RC_D0] - G[RG3] * W[RC_DXX];
+        GH1[i][RHYZ] = GH1[i][RHYZ] - G[RG2] * W[RC_DX];
+        GH1[i][RHZX] = GH1[i][RHZX] - G[RG1] * W[RC_DY];
+        GH1[i][RHZY] = GH1[i][RHZY] + G[RG1] * W[RC_DX];
+    }
+#undef AIX
+}
+
+#define RC_COMPS 15 /* 8 E slots then 7 H slots */
+
+/* calc_rc_tensor_module.F90:161-229 CalcRecalculationGreenTensor3dElement for one receiver:
+ * out[c][z] (stride Nr*Nz between components) */
+static void rc_element(const vbt_tables *t, const bkg_t *b, const anom_t *an, const rc_recv_t *rv, double xs,
+                       double ys, int lx, int ly, double dx, double dy, double complex *out, size_t comp_stride)
+{
+    int Nz = an->Nz;
+    double *WT0 = (double *)malloc(sizeof(double) * NLAM * 6);
+    double *WT = (double *)malloc(sizeof(double) * NLAM * 6);
+    double s = 1.0 / 4.0 / PI_D;
+    double x = lx * dx - dx / 2.0 + xs;
+    double y = ly * dy - dy / 2.0 + ys;
+    vbt_weights_single_int(t, x, y, dx, dy, WT0);
+    double W0 = 0.0;
+    for (int k = 0; k < NLAM; k++) {
+        WT[k * 6 + RC_D0] = WT0[k * 6 + 0];
+        WT[k * 6 + RC_DXX] = WT0[k * 6 + 1];
+        WT[k * 6 + RC_DXY] = WT0[k * 6 + 2];
+        WT[k * 6 + RC_DX] = WT0[k * 6 + 3];
+        WT[k * 6 + RC_DYY] = WT0[k * 6 + 4];
+        WT[k * 6 + RC_DY] = WT0[k * 6 + 5];
+        for (int c = 0; c < 6; c++) if (fabs(WT[k * 6 + c]) > W0) W0 = fabs(WT[k * 6 + c]);
+    }
+    double complex (*GE1)[8] = (double complex (*)[8])calloc((size_t)(Nz + 1) * 8, sizeof(double complex));
+    double complex (*GH1)[7] = (double complex (*)[7])calloc((size_t)(Nz + 1) * 7, sizeof(double complex));
+    for (int k = 0; k < NLAM; k++) {
+        double mx = 0;
+        for (int c = 0; c < 6; c++) {
+            double wm = fabs(WT[k * 6 + c] / W0);
+            if (wm > mx) mx = wm;
+        }
+        if (mx > WT_THRESHOLD) {
+            double lm = t->lms[k], W[6];
+            W[RC_DXX] = WT[k * 6 + RC_DXX] / lm;
+            W[RC_DYY] = WT[k * 6 + RC_DYY] / lm;
+            W[RC_DXY] = WT[k * 6 + RC_DXY] / lm;
+            W[RC_DX] = WT[k * 6 + RC_DX] * lm;
+            W[RC_DY] = WT[k * 6 + RC_DY] * lm;
+            W[RC_D0] = WT[k * 6 + RC_D0] * lm;
+            rc_integral_u(b, an, rv, lm, W, GE1, GH1);
+        }
+    }
+    for (int iz = 1; iz <= Nz; iz++) {
+        for (int c = 0; c < 8; c++) out[(size_t)c * comp_stride + iz - 1] = GE1[iz][c] * s;
+        for (int c = 0; c < 7; c++) out[(size_t)(8 + c) * comp_stride + iz - 1] = GH1[iz][c] * s;
+    }
+    free(GE1);
+    free(GH1);
+    free(WT);
+    free(WT0);
+}
+
+/* calc_rc_tensor_module.F90:38-159 CalcRecalculationGreenTensor over the whole 2Nx x 2Ny lag plane (all
+ * ranks' slabs): index ix < Nx is lag ix, ix > Nx is lag ix - 2Nx, ix = Nx is zero (same in y).
+ * G is [2Ny][2Nx][15][Nr][Nz]; the receivers are those of orc_prepare_receivers. */
+int orc_rc_tensor(const orc_model *m, int Nr, const double *zrecv, const double *x_shift, const double *y_shift,
+                  const int *recv_layer, const int *anom_cell, double complex *G, int nthreads)
+{
+    int Nx = m->Nx, Ny = m->Ny, Nz = m->Nz;
+    double *depth = (double *)malloc(sizeof(double) * (m->Nl + 1));
+    double complex *k2 = (double complex *)malloc(sizeof(double complex) * (m->Nl + 1));
+    bkg_t b;
+    make_bkg(m, &b, depth, k2);
+    int *L = (int *)malloc(sizeof(int) * (Nz + 1));
+    orc_layer_numbers(m, L);
+    double *dz = (double *)malloc(sizeof(double) * (Nz + 1));
+    for (int i = 1; i <= Nz; i++) dz[i] = m->z[i] - m->z[i - 1];
+    anom_t an = {Nz, L, m->z, dz};
+    vbt_tables *t = (vbt_tables *)malloc(sizeof(vbt_tables));
+    double rmin = sqrt(m->dx * m->dx + m->dy * m->dy) / 2.0; /* calc_rc_tensor_module.F90:80 */
+    vbt_init(rmin, t);
+    size_t E = (size_t)RC_COMPS * Nr * Nz;
+    memset(G, 0, sizeof(double complex) * E * 4 * Nx * Ny);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) collapse(3)
+#endif
+    for (int iy = 0; iy < 2 * Ny; iy++)
+        for (int ix = 0; ix < 2 * Nx; ix++)
+            for (int r = 0; r < Nr; r++) {
+                if (iy == Ny || ix == Nx) continue;
+                int ly = iy < Ny ? iy : iy - 2 * Ny;
+                int lx = ix < Nx ? ix : ix - 2 * Nx;
+                rc_recv_t rv = {zrecv[r], recv_layer[r], anom_cell[r]};
+                double complex *out = G + ((size_t)iy * 2 * Nx + ix) * E + (size_t)r * Nz;
+                rc_element(t, &b, &an, &rv, x_shift[r], y_shift[r], lx, ly, m->dx, m->dy, out, (size_t)Nr * Nz);
+            }
+    free(t);
+    free(dz);
+    free(L);
+    free(k2);
+    free(depth);
+    return 0;
+}
+
+/* The E and H sums of APPLY_RC_E_OP / APPLY_RC_H_OP (Continuation_Function_Module.F90:382-481) at one
+ * point: g = tensor elements [15][Nr][Nz], u = currents [3][Nz]; o[f*3+c][Nr] with f = 0 (E), 1 (H). */
+static void rc_point(int Nr, int Nz, const double complex *g, const double complex *u, double complex *o)
+{
+#define GG(c, r, z) g[((size_t)(c) * Nr + (r)) * Nz + (z)]
+    for (int r = 0; r < Nr; r++) {
+        double complex acc[6] = {0, 0, 0, 0, 0, 0};
+        for (int z = 0; z < Nz; z++) {
+            double complex ux = u[z], uy = u[Nz + z], uz = u[2 * Nz + z];
+            acc[0] += GG(REXX, r, z) * ux + GG(REXY, r, z) * uy + GG(REXZ, r, z) * uz;
+            acc[1] += GG(REXY, r, z) * ux + GG(REYY, r, z) * uy + GG(REYZ, r, z) * uz;
+            acc[2] += GG(REZX, r, z) * ux + GG(REZY, r, z) * uy + GG(REZZ, r, z) * uz;
+            acc[3] += GG(8 + RHXX, r, z) * ux + GG(8 + RHXY, r, z) * uy + GG(8 + RHXZ, r, z) * uz;
+            acc[4] += GG(8 + RHYX, r, z) * ux - GG(8 + RHXX, r, z) * uy + GG(8 + RHYZ, r, z) * uz;
+            acc[5] += GG(8 + RHZX, r, z) * ux + GG(8 + RHZY, r, z) * uy;
+        }
+        for (int o6 = 0; o6 < 6; o6++) o[(size_t)o6 * Nr + r] = acc[o6];
+    }
+#undef GG
+}
+
+/* currents j_c = (csiga - csigb(z)) E_c (LoadEint, Continuation_Function_Module.F90:240-263) as [y][x][3][Nz] */
+static double complex *rc_currents(int Nx, int Ny, int Nz, const double complex *csiga, const double complex *csigb,
+                                   const double complex *E)
+{
+    size_t cells = (size_t)Nx * Ny * Nz;
+    double complex *j = (double complex *)malloc(sizeof(double complex) * 3 * cells);
+    for (int y = 0; y < Ny; y++)
+        for (int x = 0; x < Nx; x++)
+            for (int c = 0; c < 3; c++)
+                for (int z = 0; z < Nz; z++) {
+                    size_t cell = ((size_t)z * Ny + y) * Nx + x;
+                    double complex dsig = csiga[cell] - csigb[z];
+                    j[(((size_t)y * Nx + x) * 3 + c) * Nz + z] = dsig * E[(size_t)c * cells + cell];
+                }
+    return j;
+}
+
+/* ReCalculation as direct lag sums over the spatial tensor: Ea, Ha are [Ny][Nx][3][Nr] (the reference's
+ * Ea(Nr,3,Nx,Ny)); E is the anomaly field [3][Nz][Ny][Nx]. */
+int orc_rc_apply_direct(int Nx, int Ny, int Nz, int Nr, const double complex *G, const double complex *csiga,
+                        const double complex *csigb, const double complex *E, double complex *Ea,
+                        double complex *Ha, int nthreads)
+{
+    size_t Et = (size_t)RC_COMPS * Nr * Nz;
+    double complex *j = rc_currents(Nx, Ny, Nz, csiga, csigb, E);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+#endif
+    for (int y = 0; y < Ny; y++)
+        for (int x = 0; x < Nx; x++) {
+            double complex *o = (double complex *)malloc(sizeof(double complex) * 6 * Nr);
+            double complex *acc = (double complex *)calloc((size_t)6 * Nr, sizeof(double complex));
+            for (int ys = 0; ys < Ny; ys++)
+                for (int xs = 0; xs < Nx; xs++) {
+                    int iy = (y - ys + 2 * Ny) % (2 * Ny), ix = (x - xs + 2 * Nx) % (2 * Nx);
+                    rc_point(Nr, Nz, G + ((size_t)iy * 2 * Nx + ix) * Et, j + ((size_t)ys * Nx + xs) * 3 * Nz, o);
+                    for (int k = 0; k < 6 * Nr; k++) acc[k] += o[k];
+                }
+            for (int c = 0; c < 3; c++)
+                for (int r = 0; r < Nr; r++) {
+                    Ea[(((size_t)y * Nx + x) * 3 + c) * Nr + r] = acc[(size_t)c * Nr + r];
+                    Ha[(((size_t)y * Nx + x) * 3 + c) * Nr + r] = acc[(size_t)(3 + c) * Nr + r];
+                }
+            free(acc);
+            free(o);
+        }
+    free(j);
+    return 0;
+}
+
+/* ReCalculation through the 2Nx x 2Ny FFT as the reference does it: CalcFFTofRCTensor (:330-366) on the
+ * spatial tensor, forward FFT of the currents, the point sums, backward FFT, division by 4NxNy (:324-328),
+ * crop to the physical grid. */
+int orc_rc_apply_fft(int Nx, int Ny, int Nz, int Nr, const double complex *G, const double complex *csiga,
+                     const double complex *csigb, const double complex *E, double complex *Ea, double complex *Ha,
+                     int nthreads)
+{
+    int n1 = 2 * Nx, n2 = 2 * Ny;
+    size_t npts = (size_t)n1 * n2, Et = (size_t)RC_COMPS * Nr * Nz;
+    double complex *Gh = (double complex *)malloc(sizeof(double complex) * npts * Et);
+    double complex *U = (double complex *)calloc(npts * 3 * Nz, sizeof(double complex));
+    double complex *O = (double complex *)malloc(sizeof(double complex) * npts * 6 * Nr);
+    double complex *j = rc_currents(Nx, Ny, Nz, csiga, csigb, E);
+    for (int y = 0; y < Ny; y++)
+        for (int x = 0; x < Nx; x++)
+            memcpy(U + ((size_t)y * n1 + x) * 3 * Nz, j + ((size_t)y * Nx + x) * 3 * Nz, sizeof(double complex) * 3 * Nz);
+    free(j);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    /* element-wise 2-D transforms: plane[iy][ix] of one element */
+#define RC_FFT_ELEMS(buf, ne, sign)                                                                       \
+    do {                                                                                                  \
+        _Pragma("omp parallel") {                                                                         \
+            double complex *plane = (double complex *)malloc(sizeof(double complex) * npts);              \
+            double complex *work = (double complex *)malloc(sizeof(double complex) * (n1 > n2 ? n1 : n2)); \
+            _Pragma("omp for schedule(dynamic, 4)") for (size_t e = 0; e < (size_t)(ne); e++) {           \
+                for (size_t p = 0; p < npts; p++) plane[p] = (buf)[p * (ne) + e];                         \
+                fft2d(plane, n1, n2, (sign), work);                                                       \
+                for (size_t p = 0; p < npts; p++) (buf)[p * (ne) + e] = plane[p];                         \
+            }                                                                                             \
+            free(work);                                                                                   \
+            free(plane);                                                                                  \
+        }                                                                                                 \
+    } while (0)
+    memcpy(Gh, G, sizeof(double complex) * npts * Et);
+    RC_FFT_ELEMS(Gh, Et, -1);
+    RC_FFT_ELEMS(U, (size_t)3 * Nz, -1);
+    for (size_t p = 0; p < npts; p++) rc_point(Nr, Nz, Gh + p * Et, U + p * 3 * Nz, O + p * 6 * Nr);
+    RC_FFT_ELEMS(O, (size_t)6 * Nr, 1);
+#undef RC_FFT_ELEMS
+    double complex nrm = (double)(4 * Nx * Ny);
+    for (int y = 0; y < Ny; y++)
+        for (int x = 0; x < Nx; x++)
+            for (int c = 0; c < 3; c++)
+                for (int r = 0; r < Nr; r++) {
+                    const double complex *o = O + ((size_t)y * n1 + x) * 6 * Nr;
+                    Ea[(((size_t)y * Nx + x) * 3 + c) * Nr + r] = o[(size_t)c * Nr + r] / nrm;
+                    Ha[(((size_t)y * Nx + x) * 3 + c) * Nr + r] = o[(size_t)(3 + c) * Nr + r] / nrm;
+                }
+    free(O);
+    free(U);
+    free(Gh);
+    return 0;
+}
+
+/* sources_module.F90:26-66 PlaneWave: normal field at receiver depths, F[Nr][6] = Ex Ey Ez Hx Hy Hz;
+ * pol 0 = EX, 1 = EY */
+int orc_plane_wave_points(const orc_model *m, int pol, int Nr, const double *zrecv, double complex *F)
+{
+    int Nl = m->Nl;
+    double depth[Nl + 1];
+    double complex k2[Nl + 1];
+    bkg_t b;
+    make_bkg(m, &b, depth, k2);
+    double complex Arr[Nl + 1][2], p[Nl + 1][2], q[Nl + 1][2], eta[Nl + 1];
+    double complex *A = (double complex *)calloc((size_t)(Nl + 1) * (Nl + 1) * 2, sizeof(double complex));
+    calc_apq(&b, 0.0, Arr, p, q, eta, A);
+#define AIX(i, j, k) A[(((size_t)(i) * (Nl + 1)) + (j)) * 2 + (k)]
+    double complex t1 = Nl > 1 ? 1.0 + q[1][0] * cexp(-b.depth[1] * eta[1] * 2.0) : 1.0;
+    t1 = AIX(1, 1, 0) * t1;
+    memset(F, 0, sizeof(double complex) * 6 * Nr);
+    for (int ir = 0; ir < Nr; ir++) {
+        int l = orc_get_layer(zrecv[ir], Nl, depth);
+        if (l < 1) l = 1;
+        double complex t2 = AIX(l, 1, 0) / t1;
+        double complex e1 = cexp(-eta[l] * zrecv[ir]);
+        double complex e2 = l < Nl ? q[l][0] * (cexp(-eta[l] * (2.0 * b.depth[l] - zrecv[ir]))) : 0.0;
+        double complex g1 = t2 * (e1 + e2);
+        double complex g2 = -t2 * (e1 - e2) * eta[l] / b.iwm;
+        if (pol == 0) {
+            F[ir * 6 + 0] = g1;
+            F[ir * 6 + 4] = g2;
+        } else {
+            F[ir * 6 + 1] = g1;
+            F[ir * 6 + 3] = -g2;
+        }
+    }
+#undef AIX
+    free(A);
     return 0;
 }

@@ -103,6 +103,26 @@ void orc_set_anomaly_sigma(int Nx, int Ny, int Nz, const double *siga_zxy, doubl
 void orc_set_freq(int Nl, const double *sigma, double freq, int displacement_currents,
                   double complex *csigma /* Nl+1 */);
 
+/* Receiver continuation (Continuation_Function_Module.F90, calc_rc_tensor_module.F90,
+ * rc_kernel_hankel_module.F90).  Receivers: depth zrecv (moved to the top of its cell when strictly inside
+ * one), lateral shifts x_shift, y_shift, layer and anom_cell from orc_prepare_receivers.
+ * Tensor layout [2Ny][2Nx][15][Nr][Nz]: lag index ix < Nx is lag ix, ix > Nx is ix - 2Nx, ix = Nx is zero
+ * (same in y); components E: xx xy xz yy yz zx zy zz, then H: xx xy xz yx yz zx zy.
+ * Fields at receivers: Ea, Ha [Ny][Nx][3][Nr] (the reference's Ea(Nr,3,Nx,Ny)). */
+int orc_prepare_receivers(const orc_model *m, int Nr, double *zrecv, int *recv_layer, int *anom_cell);
+int orc_vbt_weights_single(double x, double y, double hx, double hy, double rmin,
+                           double *WT /* [501][6] */, double *lms /* [501] */);
+int orc_rc_tensor(const orc_model *m, int Nr, const double *zrecv, const double *x_shift, const double *y_shift,
+                  const int *recv_layer, const int *anom_cell, double complex *G, int nthreads);
+int orc_rc_apply_direct(int Nx, int Ny, int Nz, int Nr, const double complex *G, const double complex *csiga,
+                        const double complex *csigb, const double complex *E, double complex *Ea,
+                        double complex *Ha, int nthreads);
+int orc_rc_apply_fft(int Nx, int Ny, int Nz, int Nr, const double complex *G, const double complex *csiga,
+                     const double complex *csigb, const double complex *E, double complex *Ea, double complex *Ha,
+                     int nthreads);
+/* PlaneWave (sources_module.F90:26-66) at receiver depths: F[Nr][6] = Ex Ey Ez Hx Hy Hz; pol 0 EX, 1 EY */
+int orc_plane_wave_points(const orc_model *m, int pol, int Nr, const double *zrecv, double complex *F);
+
 double orc_eps0(void);
 double orc_mu0(void);
 
