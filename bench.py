@@ -406,6 +406,39 @@ def run_b200(args, rank, world, local_rank):
     ach64 = B64 / (ms64 * 1e-3) / 1e9
     ach32 = B32 / (ms32 * 1e-3) / 1e9
 
+    # receiver fields (the reference's "Recalculate Fields") for one line of surface receivers on this grid:
+    # receiver tensor build + its spectrum (once per frequency) and one recalculation (per solution)
+    def time_receivers(reps=10):
+        rcop = g2.RCOperator.from_model(m, [0.0])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rcop.calc_rc_kernel(m.csigma, m.thick, m.omega)
+        t1 = time.perf_counter()
+        rcop.calc_fft_of_rc_kernel()
+        t2 = time.perf_counter()
+        rcop.set_anomaly_sigma(sig, m.freq)
+        E = torch.randn(n, dtype=torch.complex128, device=dev)
+        Ea = torch.empty(3 * m.Nx * m.Ny, dtype=torch.complex128, device=dev)
+        Ha = torch.empty_like(Ea)
+        rst = torch.cuda.ExternalStream(rcop.stream)
+        for _ in range(3):
+            rcop.recalculate_device(E.data_ptr(), Ea.data_ptr(), Ha.data_ptr())
+        torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(rst)
+        for _ in range(reps):
+            rcop.recalculate_device(E.data_ptr(), Ea.data_ptr(), Ha.data_ptr())
+        r1.record(rst)
+        torch.cuda.synchronize()
+        ms = r0.elapsed_time(r1) / reps
+        rcop.delete()
+        tb = 4 * m.Nx * m.Ny * 15 * m.Nz * 16  # spectral receiver tensor, read once per recalculation
+        io = 16 * (n + 2 * 3 * m.Nx * m.Ny + m.Nx * m.Ny * m.Nz)  # E in, Ea and Ha out, dsig
+        return {"receivers": 1, "tensor_build_s": t1 - t0, "tensor_fft_s": t2 - t1, "recalculate_ms": ms,
+                "bytes_per_recalculate": tb + io, "achieved_gbs": (tb + io) / (ms * 1e-3) / 1e9}
+
+    rcv = time_receivers() if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -457,6 +490,7 @@ def run_b200(args, rank, world, local_rank):
                       "true_rel_residual_mixed": [iy.be, ix.be],
                       "field_error_vs_fp64_tol1e-8": [err_y, err_x]},
             "learned_preconditioner": learned,
+            "receiver_fields": rcv,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }

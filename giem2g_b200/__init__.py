@@ -78,6 +78,9 @@ EXPORTED_SYMBOLS = [
     "giem2g_apply_ie_operator_device_batch", "giem2g_gemm_bf16_tn", "giem2g_im2col3d_bf16",
     "giem2g_col2im3d_f32", "giem2g_set_outer_preconditioner", "giem2g_set_fft_lines",
     "giem2g_set_kernel_timing", "giem2g_last_contract_ms",
+    "giem2g_rc_create", "giem2g_rc_receivers", "giem2g_rc_calc_kernel", "giem2g_rc_calc_fft_of_kernel",
+    "giem2g_rc_get_kernel", "giem2g_rc_set_anomaly_conductivity", "giem2g_rc_recalculate",
+    "giem2g_rc_recalculate_device", "giem2g_rc_get_stream", "giem2g_rc_delete",
 ]
 
 
@@ -147,6 +150,19 @@ def lib():
     L.giem2g_set_kernel_timing.argtypes = [vp, ip]
     L.giem2g_last_contract_ms.argtypes = [vp]
     L.giem2g_last_contract_ms.restype = dp
+    L.giem2g_rc_create.argtypes = [BackgroundT, AnomalyT, ip, vp, vp, vp]
+    L.giem2g_rc_create.restype = vp
+    L.giem2g_rc_receivers.argtypes = [vp, vp, vp, vp]
+    L.giem2g_rc_calc_kernel.argtypes = [vp, BackgroundT, dp]
+    L.giem2g_rc_calc_fft_of_kernel.argtypes = [vp]
+    L.giem2g_rc_get_kernel.argtypes = [vp, vp]
+    L.giem2g_rc_set_anomaly_conductivity.argtypes = [vp, vp]
+    L.giem2g_rc_recalculate.argtypes = [vp, vp, vp, vp]
+    L.giem2g_rc_recalculate_device.argtypes = [vp, vp, vp, vp]
+    L.giem2g_rc_get_stream.argtypes = [vp]
+    L.giem2g_rc_get_stream.restype = vp
+    L.giem2g_rc_delete.argtypes = [vp]
+    L.giem2g_rc_delete.restype = None
     _lib = L
     return L
 
@@ -361,6 +377,107 @@ class IEOperator:
     def delete(self):
         if self.handle:
             lib().giem2g_delete_ie_operator(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass
+
+
+class RCOperator:
+    """Receiver continuation on the current CUDA device (RC_OPERATOR, Continuation_Function_Module.F90).
+
+    Receivers: depths zrecv with lateral shifts; receiver r at anomaly cell (ix, iy) is the point
+    ((ix+1/2) dx + x_shift, (iy+1/2) dy + y_shift, zrecv).  Fields at the receivers come back as
+    complex [Ny, Nx, 3, Nr] (the reference's Ea(Nr,3,Nx,Ny)).
+
+      RCOperator(...)            PrepareRecvs + PrepareContinuationOperator
+      calc_rc_kernel             CalcRecalculationGreenTensor (calc_rc_tensor_module.F90:38)
+      calc_fft_of_rc_kernel      CalcFFTofRCTensor (Continuation_Function_Module.F90:330)
+      set_anomaly_sigma          FinalizeRCOperator (:165)
+      recalculate                ReCalculation (:198): anomalous E and H at the receivers
+    """
+
+    def __init__(self, Nx, Ny, Nz, dx, dy, z, thick, zrecv, x_shift=None, y_shift=None):
+        self.Nx, self.Ny, self.Nz = int(Nx), int(Ny), int(Nz)
+        self.dx, self.dy = float(dx), float(dy)
+        self._z = np.ascontiguousarray(z, dtype=np.float64)
+        self._dz = np.ascontiguousarray(np.diff(self._z), dtype=np.float64)
+        self._anom = AnomalyT(self.Nx, self.Ny, self.Nz, self.dx, self.dy, self._z.ctypes.data, self._dz.ctypes.data)
+        zr = np.ascontiguousarray(np.atleast_1d(zrecv), dtype=np.float64)
+        self.Nr = len(zr)
+        xs = np.ascontiguousarray(np.zeros(self.Nr) if x_shift is None else x_shift, dtype=np.float64)
+        ys = np.ascontiguousarray(np.zeros(self.Nr) if y_shift is None else y_shift, dtype=np.float64)
+        self.x_shift, self.y_shift = xs, ys
+        th = np.ascontiguousarray(thick, dtype=np.float64) if len(thick) else np.zeros(1)
+        cs = np.zeros(len(thick) + 2, np.complex128)  # values unused here: only the layer depths
+        bkg = BackgroundT(len(thick) + 1, cs.ctypes.data, th.ctypes.data)
+        self.handle = lib().giem2g_rc_create(bkg, self._anom, self.Nr, zr.ctypes.data, xs.ctypes.data, ys.ctypes.data)
+        if not self.handle:
+            _check(what="giem2g_rc_create")
+            raise Giem2gError("giem2g_rc_create failed")
+        self._keep = []
+
+    @classmethod
+    def from_model(cls, m, zrecv, x_shift=None, y_shift=None):
+        return cls(m.Nx, m.Ny, m.Nz, m.dx, m.dy, m.z, m.thick, zrecv, x_shift, y_shift)
+
+    def receivers(self):
+        """(depths used, receiver layers, anomaly cells above each receiver) after PrepareRecvs."""
+        z = np.zeros(self.Nr)
+        rl = np.zeros(self.Nr, np.int32)
+        ac = np.zeros(self.Nr, np.int32)
+        _check(lib().giem2g_rc_receivers(self.handle, z.ctypes.data, rl.ctypes.data, ac.ctypes.data), "rc_receivers")
+        return z, rl, ac
+
+    def calc_rc_kernel(self, csigma, thick, omega):
+        cs = _c128(csigma)
+        th = np.ascontiguousarray(thick, dtype=np.float64) if len(thick) else np.zeros(1)
+        self._keep = [cs, th]
+        bkg = BackgroundT(len(cs) - 1, cs.ctypes.data, th.ctypes.data)
+        _check(lib().giem2g_rc_calc_kernel(self.handle, bkg, float(omega)), "giem2g_rc_calc_kernel")
+
+    def calc_fft_of_rc_kernel(self):
+        _check(lib().giem2g_rc_calc_fft_of_kernel(self.handle), "giem2g_rc_calc_fft_of_kernel")
+
+    def get_kernel(self):
+        """The current tensor (spatial or spectral): complex [2Ny, 2Nx, 15, Nr, Nz]."""
+        G = np.zeros((2 * self.Ny, 2 * self.Nx, 15, self.Nr, self.Nz), np.complex128)
+        _check(lib().giem2g_rc_get_kernel(self.handle, G.ctypes.data), "giem2g_rc_get_kernel")
+        return G
+
+    def set_anomaly_conductivity(self, csiga):
+        """csiga: complex [Nz,Ny,Nx] at the kernel's frequency."""
+        c = _c128(csiga)
+        assert c.size == self.Nx * self.Ny * self.Nz
+        _check(lib().giem2g_rc_set_anomaly_conductivity(self.handle, c.ctypes.data), "rc_set_anomaly_conductivity")
+
+    def set_anomaly_sigma(self, siga_file_order, freq, displacement_currents=True):
+        from .synthetic import csiga_from_sigma
+        self.set_anomaly_conductivity(csiga_from_sigma(siga_file_order, freq, displacement_currents))
+
+    def recalculate(self, E):
+        """E [3,Nz,Ny,Nx] (an IE solution) -> anomalous (Ea, Ha), each complex [Ny, Nx, 3, Nr]."""
+        Ei = _c128(E)
+        assert Ei.size == 3 * self.Nx * self.Ny * self.Nz
+        Ea = np.zeros((self.Ny, self.Nx, 3, self.Nr), np.complex128)
+        Ha = np.zeros_like(Ea)
+        _check(lib().giem2g_rc_recalculate(self.handle, Ei.ctypes.data, Ea.ctypes.data, Ha.ctypes.data),
+               "giem2g_rc_recalculate")
+        return Ea, Ha
+
+    def recalculate_device(self, d_E: int, d_Ea: int, d_Ha: int):
+        _check(lib().giem2g_rc_recalculate_device(self.handle, d_E, d_Ea, d_Ha), "giem2g_rc_recalculate_device")
+
+    @property
+    def stream(self) -> int:
+        return lib().giem2g_rc_get_stream(self.handle)
+
+    def delete(self):
+        if self.handle:
+            lib().giem2g_rc_delete(self.handle)
             self.handle = None
 
     def __del__(self):

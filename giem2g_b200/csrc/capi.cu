@@ -3,12 +3,14 @@
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
 #include "common.cuh"
 #include "ie_internal.h"
 #include "krylov.h"
+#include "rc_internal.h"
 
 namespace {
 std::mutex g_mu;
@@ -665,6 +667,153 @@ void giem2g_print_stats(void *ie)
     g2_log("===================================================================================");
     op->mult_num = 0;
     op->apply_seconds = 0;
+}
+
+// ---- receiver continuation (Continuation_Function_Module.F90; no C interface in the reference) ----
+
+// depth[1..Nl-1] of a background (giem2g_interfaces.F90:264-268)
+static std::vector<double> bkg_depth(const GIEM2G_BACKGROUND_TYPE &bkg)
+{
+    std::vector<double> depth(bkg.Nl + 1, 0.0);
+    if (bkg.Nl > 1) {
+        const double *th = reinterpret_cast<const double *>(bkg.thickness);
+        depth[1] = th[0];
+        for (int i = 2; i <= bkg.Nl - 1; i++) depth[i] = depth[i - 1] + th[i - 1];
+    }
+    return depth;
+}
+
+void *giem2g_rc_create(GIEM2G_BACKGROUND_TYPE bkg, GIEM2G_ANOMALY_TYPE anomaly, int Nr, const double *zrecv,
+                       const double *x_shift, const double *y_shift)
+{
+    const int Nx = anomaly.Nx, Ny = anomaly.Ny, Nz = anomaly.Nz;
+    if (Nx <= 0 || Ny <= 0 || Nz <= 0 || !is_pow2(2 * Nx) || !is_pow2(2 * Ny) || 2 * Nx > 2048 || 2 * Ny > 2048 ||
+        !anomaly.z) {
+        fail(G2_ERR_ARG, "giem2g_rc_create: Nx and Ny must be powers of two up to 1024");
+        return nullptr;
+    }
+    if (Nr < 1 || !zrecv || bkg.Nl < 1 || (bkg.Nl > 1 && !bkg.thickness)) {
+        fail(G2_ERR_ARG, "giem2g_rc_create: no receivers or bad background");
+        return nullptr;
+    }
+    const double *z = reinterpret_cast<const double *>(anomaly.z);
+    const std::vector<double> depth = bkg_depth(bkg);
+    // PrepareRecvs (data_types_module.F90:124-152)
+    std::vector<RcReceiver> rv(Nr);
+    for (int i = 0; i < Nr; i++) {
+        const double zr = zrecv[i];
+        RcReceiver &r = rv[i];
+        r.zrecv = zr;
+        r.x_shift = x_shift ? x_shift[i] : 0.0;
+        r.y_shift = y_shift ? y_shift[i] : 0.0;
+        r.recv_layer = std::max(get_layer(zr, bkg.Nl, depth), 1);
+        if (zr <= z[0]) {
+            r.anom_cell = 0;
+        } else if (zr >= z[Nz]) {
+            r.anom_cell = Nz + 1;
+        } else {
+            for (int iz = 1; iz <= Nz; iz++) {
+                if (std::fabs(zr / z[iz] - 1.0) < 1e-7) {
+                    r.anom_cell = iz;
+                    break;
+                } else if (zr > z[iz - 1] && zr < z[iz]) {
+                    r.zrecv = z[iz - 1];  // moved to the top border of its cell
+                    r.anom_cell = iz - 1;
+                    break;
+                }
+            }
+        }
+    }
+    RcOp *op = rc_create(Nx, Ny, Nz, anomaly.dx, anomaly.dy, z, Nr, rv.data());
+    if (!op) {
+        fail(G2_ERR_NOMEM, "giem2g_rc_create: %s", giem2g_last_error());
+        return nullptr;
+    }
+    set_status(0);
+    return op;
+}
+
+int giem2g_rc_receivers(void *rc, double *zrecv, int *recv_layer, int *anom_cell)
+{
+    if (!rc) return fail(G2_ERR_STATE, "giem2g_rc_receivers: no operator");
+    RcOp *op = reinterpret_cast<RcOp *>(rc);
+    std::vector<RcReceiver> rv(rc_count(op));
+    rc_receivers(op, rv.data());
+    for (size_t i = 0; i < rv.size(); i++) {
+        if (zrecv) zrecv[i] = rv[i].zrecv;
+        if (recv_layer) recv_layer[i] = rv[i].recv_layer;
+        if (anom_cell) anom_cell[i] = rv[i].anom_cell;
+    }
+    return set_status(0);
+}
+
+int giem2g_rc_calc_kernel(void *rc, GIEM2G_BACKGROUND_TYPE bkg, double omega)
+{
+    if (!rc) return fail(G2_ERR_STATE, "giem2g_rc_calc_kernel: no operator");
+    if (bkg.Nl < 1 || !bkg.csigb || (bkg.Nl > 1 && !bkg.thickness)) return fail(G2_ERR_ARG, "giem2g_rc_calc_kernel: bad background");
+    RcOp *op = reinterpret_cast<RcOp *>(rc);
+    // Lnumber (giem2g_interfaces.F90:163-165) from the operator's cell borders
+    const int Nz = rc_nz(op);
+    const double *z = rc_borders(op);
+    const std::vector<double> depth = bkg_depth(bkg);
+    std::vector<int> L(Nz + 1);
+    for (int i = 1; i <= Nz; i++) L[i] = get_layer((z[i - 1] + z[i]) / 2.0, bkg.Nl, depth);
+    L[0] = get_layer(z[0] * (1.0 - 1e-7), bkg.Nl, depth);
+    for (int i = 1; i <= Nz; i++)
+        if (L[i] < 1) return fail(G2_ERR_ARG, "giem2g_rc_calc_kernel: anomaly cell %d is not below the surface", i);
+    std::vector<RcReceiver> rv(rc_count(op));
+    rc_receivers(op, rv.data());
+    for (const RcReceiver &r : rv)
+        if (r.recv_layer > bkg.Nl)
+            return fail(G2_ERR_ARG, "giem2g_rc_calc_kernel: receivers were prepared for a background with more layers");
+    std::vector<double> th;
+    if (bkg.Nl > 1) th.assign(reinterpret_cast<const double *>(bkg.thickness),
+                              reinterpret_cast<const double *>(bkg.thickness) + bkg.Nl - 1);
+    return set_status(rc_calc_kernel(op, bkg.Nl, reinterpret_cast<const double2 *>(bkg.csigb), th.data(), omega,
+                                     L.data()));
+}
+
+int giem2g_rc_calc_fft_of_kernel(void *rc)
+{
+    if (!rc) return fail(G2_ERR_STATE, "giem2g_rc_calc_fft_of_kernel: no operator");
+    return set_status(rc_fft_kernel(reinterpret_cast<RcOp *>(rc)));
+}
+
+int giem2g_rc_get_kernel(void *rc, void *G)
+{
+    if (!rc || !G) return fail(G2_ERR_ARG, "giem2g_rc_get_kernel: null argument");
+    return set_status(rc_copy_kernel(reinterpret_cast<RcOp *>(rc), reinterpret_cast<double2 *>(G)));
+}
+
+int giem2g_rc_set_anomaly_conductivity(void *rc, const void *csiga)
+{
+    if (!rc || !csiga) return fail(G2_ERR_ARG, "giem2g_rc_set_anomaly_conductivity: null argument");
+    return set_status(rc_set_anomaly_conductivity(reinterpret_cast<RcOp *>(rc), reinterpret_cast<const double2 *>(csiga)));
+}
+
+int giem2g_rc_recalculate(void *rc, const void *E, void *Ea, void *Ha)
+{
+    if (!rc || !E || !Ea || !Ha) return fail(G2_ERR_ARG, "giem2g_rc_recalculate: null argument");
+    return set_status(rc_recalculate_host(reinterpret_cast<RcOp *>(rc), reinterpret_cast<const double2 *>(E),
+                                          reinterpret_cast<double2 *>(Ea), reinterpret_cast<double2 *>(Ha)));
+}
+
+int giem2g_rc_recalculate_device(void *rc, const void *d_E, void *d_Ea, void *d_Ha)
+{
+    if (!rc || !d_E || !d_Ea || !d_Ha) return fail(G2_ERR_ARG, "giem2g_rc_recalculate_device: null argument");
+    return set_status(rc_recalculate_device(reinterpret_cast<RcOp *>(rc), reinterpret_cast<const double2 *>(d_E),
+                                            reinterpret_cast<double2 *>(d_Ea), reinterpret_cast<double2 *>(d_Ha)));
+}
+
+void *giem2g_rc_get_stream(void *rc)
+{
+    return rc ? reinterpret_cast<void *>(rc_stream(reinterpret_cast<RcOp *>(rc))) : nullptr;
+}
+
+void giem2g_rc_delete(void *rc)
+{
+    rc_delete(reinterpret_cast<RcOp *>(rc));
+    set_status(0);
 }
 
 void giem2g_delete_ie_operator(void *ie)

@@ -10,7 +10,13 @@
   siga(Nz, Nx, Ny), z fastest; numbers separated by blanks, commas or new lines, with optional
   ``r*value`` repeat counts and D exponents.  Returned as numpy [Ny, Nx, Nz].
 * Input JSON (mpi_saveload_module.F90:30-239): the reference's keys, read leniently (trailing commas,
-  which the reference's own parser accepts, are allowed).
+  which the reference's own parser accepts, are allowed).  Receivers come from "Recievers" (the
+  reference's spelling): a list of {"depth", "xshift", "yshift"} (LoadRecievers, :174-213).
+* Receiver output (SaveOutputOneFile, mpi_saveload_module.F90:391-483): ``P{Y,X}_F<freq>.dat``, a title
+  line "%" + 28 A20 titles, then one line per receiver and cell (receiver outer, then y, then x) of
+  " " + 28 ES20.10E3 numbers: x, y, z of the receiver, frequency, then Re/Im of Ea (Ex Ey Ez),
+  Ha (Hx Hy Hz), Et, Ht.  The receiver at cell (ix, iy) (0-based) is at x = (ix + 1/2) dx + xshift,
+  y = (iy + 1/2) dy + yshift.
 """
 from __future__ import annotations
 
@@ -80,3 +86,53 @@ def load_input(path: str) -> dict:
     text = open(path).read()
     text = re.sub(r",(\s*[\]}])", r"\1", text)
     return json.loads(text)
+
+
+def receiver_output_name(pol: int, freq: float) -> str:
+    """PY_F<freq>.dat for pol EY, PX_F<freq>.dat for pol EX (giem2g.F90:427-428, :501-502)."""
+    return ("PY_F" if pol == EY else "PX_F") + freq_string(freq) + ".dat"
+
+
+_TITLES = ["x_recv", "y_recv", "z_recv", "frequency",
+           "Re Ex^a", "Im Ex^a", "Re Ey^a", "Im Ey^a", "Re Ez^a", "Im Ez^a",
+           "Re Hx^a", "Im Hx^a", "Re Hy^a", "Im Hy^a", "Re Hz^a", "Im Hz^a",
+           "Re Ex^t", "Im Ex^t", "Re Ey^t", "Im Ey^t", "Re Ez^t", "Im Ez^t",
+           "Re Hx^t", "Im Hx^t", "Re Hy^t", "Im Hy^t", "Re Hz^t", "Im Hz^t"]
+
+
+def _es20_10e3(v: float) -> str:
+    """Fortran ES20.10E3: one digit before the point, ten after, a three-digit exponent."""
+    mant, exp = f"{float(v):.10E}".split("E")
+    return f"{mant}E{int(exp):+04d}".rjust(20)
+
+
+def save_receiver_fields(path: str, dx: float, dy: float, zrecv, x_shift, y_shift, freq: float,
+                         Ea: np.ndarray, Ha: np.ndarray, Et: np.ndarray, Ht: np.ndarray) -> None:
+    """Fields [Ny, Nx, 3, Nr] (the reference's (Nr,3,Nx,Ny)) -> the reference's text table."""
+    Ny, Nx, _, Nr = Ea.shape
+    lines = ["%" + "".join(t.rjust(20) for t in _TITLES)]
+    for r in range(Nr):
+        for iy in range(Ny):
+            y = (iy + 1) * dy - dy / 2.0 + y_shift[r]
+            for ix in range(Nx):
+                x = (ix + 1) * dx - dx / 2.0 + x_shift[r]
+                vals = [x, y, zrecv[r], freq]
+                for F in (Ea, Ha, Et, Ht):
+                    for c in range(3):
+                        v = F[iy, ix, c, r]
+                        vals += [v.real, v.imag]
+                lines.append(" " + "".join(_es20_10e3(v) for v in vals))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
+def load_receiver_fields(path: str) -> np.ndarray:
+    """The numeric table of a receiver output file: [rows, 28] (x, y, z, f, then 24 Re/Im values)."""
+    return np.loadtxt(path, comments="%", ndmin=2)
+
+
+def receivers_from_input(inp: dict):
+    """(depths, xshifts, yshifts) from the "Recievers" list of the input JSON."""
+    rs = inp.get("Recievers", [])
+    return ([float(r["depth"]) for r in rs], [float(r.get("xshift", 0.0)) for r in rs],
+            [float(r.get("yshift", 0.0)) for r in rs])

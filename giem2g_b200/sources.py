@@ -1,8 +1,10 @@
-"""Plane-wave source: cell-averaged 1-D background field, the right-hand side of the IE solve.
+"""Plane-wave source: the 1-D background (normal) field of the layered medium.
 
-Restates PlaneWaveIntegral (sources_module.F90:67-101) with the lambda = 0 layered recursion of
-Calc_APQ (apq_module.F90:230-312).  The field is constant in x and y; only the polarisation's
-component is nonzero.  Host-side numpy: it is a handful of complex numbers per layer and cell.
+Restates PlaneWaveIntegral (sources_module.F90:67-101), the cell-averaged field that is the
+right-hand side of the IE solve, and PlaneWave (:26-66), the field at receiver depths that the
+receiver fields add to the anomalous part, both with the lambda = 0 layered recursion of Calc_APQ
+(apq_module.F90:230-312).  The field is constant in x and y.  Host-side numpy: it is a handful of
+complex numbers per layer and cell.
 """
 from __future__ import annotations
 
@@ -13,37 +15,38 @@ from .synthetic import MU0
 EX, EY = 0, 1
 
 
-def _layer_numbers(m) -> np.ndarray:
-    """Lnumber(0:Nz) (mpi_saveload_module.F90:99-100, data_types_module.F90:214-242)."""
+def get_layer(m, z) -> int:
+    """GetLayerSingle (data_types_module.F90:214-242): 0 at the surface, -1 in the air."""
     depth = np.r_[0.0, np.cumsum(m.thick)]  # depth[1..Nl-1]
+    if abs(z) < 1e-15:
+        return 0
+    if z < 0:
+        return -1
+    if m.Nl == 1:
+        return 1
+    if z > depth[m.Nl - 1]:
+        return m.Nl
+    l = 1
+    while z > depth[l]:
+        l += 1
+    return l
 
-    def get_layer(z):
-        if abs(z) < 1e-15:
-            return 0
-        if z < 0:
-            return -1
-        if m.Nl == 1:
-            return 1
-        if z > depth[m.Nl - 1]:
-            return m.Nl
-        l = 1
-        while z > depth[l]:
-            l += 1
-        return l
 
+def _layer_numbers(m) -> np.ndarray:
+    """Lnumber(0:Nz) (mpi_saveload_module.F90:99-100)."""
     L = np.zeros(m.Nz + 1, int)
     for i in range(1, m.Nz + 1):
-        L[i] = get_layer(0.5 * (m.z[i - 1] + m.z[i]))
-    L[0] = get_layer(m.z[0] * (1.0 - 1e-7))
+        L[i] = get_layer(m, 0.5 * (m.z[i - 1] + m.z[i]))
+    L[0] = get_layer(m, m.z[0] * (1.0 - 1e-7))
     return L
 
 
-def plane_wave_integral(m, pol: int) -> np.ndarray:
-    """E0[3, Nz, Ny, Nx] (Fortran (Nx,Ny,Nz,3)); pol 0 = EX, 1 = EY."""
+def _apq0(m):
+    """Calc_APQ at lambda = 0 (apq_module.F90:230-312): eta, q, depth, A(l,1,1) and the surface factor t1
+    of PlaneWave / PlaneWaveIntegral (sources_module.F90:36-42, :78-84)."""
     Nl = m.Nl
     cs = m.csigma
     k2 = 1j * cs * MU0 * m.omega
-    iwm = 1j * MU0 * m.omega  # noqa: F841  (only the electric field is needed)
     thick = np.r_[0.0, m.thick]
     depth = np.r_[0.0, np.cumsum(m.thick)]
     eta = np.zeros(Nl + 1, complex)
@@ -84,6 +87,13 @@ def plane_wave_integral(m, pol: int) -> np.ndarray:
         A11[i] = v
     t1 = 1 + q[1, 0] * np.exp(-depth[1] * eta[1] * 2) if Nl > 1 else 1.0 + 0j
     t1 = A11[1] * t1
+    return eta, q, depth, A11, t1
+
+
+def plane_wave_integral(m, pol: int) -> np.ndarray:
+    """E0[3, Nz, Ny, Nx] (Fortran (Nx,Ny,Nz,3)); pol 0 = EX, 1 = EY."""
+    Nl = m.Nl
+    eta, q, depth, A11, t1 = _apq0(m)
     L = _layer_numbers(m)
     E0 = np.zeros((3, m.Nz, m.Ny, m.Nx), complex)
     for iz in range(1, m.Nz + 1):
@@ -100,3 +110,25 @@ def plane_wave_integral(m, pol: int) -> np.ndarray:
         G = G / dz / eta[l]
         E0[pol, iz - 1] = G
     return E0
+
+
+def plane_wave_points(m, pol: int, zrecv) -> np.ndarray:
+    """PlaneWave (sources_module.F90:26-66): the normal field at receiver depths, F[Nr, 6] with columns
+    Ex Ey Ez Hx Hy Hz; pol 0 = EX (Ex, Hy nonzero), 1 = EY (Ey, Hx nonzero)."""
+    Nl = m.Nl
+    eta, q, depth, A11, t1 = _apq0(m)
+    iwm = 1j * MU0 * m.omega
+    zr = np.atleast_1d(np.asarray(zrecv, dtype=np.float64))
+    F = np.zeros((len(zr), 6), complex)
+    for ir, z in enumerate(zr):
+        l = max(get_layer(m, z), 1)
+        t2 = A11[l] / t1
+        e1 = np.exp(-eta[l] * z)
+        e2 = q[l, 0] * np.exp(-eta[l] * (2.0 * depth[l] - z)) if l < Nl else 0.0
+        g1 = t2 * (e1 + e2)
+        g2 = -t2 * (e1 - e2) * eta[l] / iwm
+        if pol == EX:
+            F[ir, 0], F[ir, 4] = g1, g2
+        else:
+            F[ir, 1], F[ir, 3] = g1, -g2
+    return F

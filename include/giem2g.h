@@ -204,6 +204,42 @@ int giem2g_im2col3d_bf16(const void *x, void *cols, int N, int D, int H, int W, 
 int giem2g_col2im3d_f32(const float *dcols, float *dx, int N, int D, int H, int W, int C, int stride, int Kp,
                         void *stream);
 
+/* ---- receiver continuation ---------------------------------------------------------------------
+ * Fields at receiver points from the currents j = (csiga - csigb) E of an IE solution.  The reference
+ * has no C interface for this part; these entry points follow its Fortran module routines:
+ *   giem2g_rc_create             PrepareRecvs (data_types_module.F90:124-152) +
+ *                                PrepareContinuationOperator (Continuation_Function_Module.F90:84-164)
+ *   giem2g_rc_calc_kernel        CalcRecalculationGreenTensor (calc_rc_tensor_module.F90:38-229)
+ *   giem2g_rc_calc_fft_of_kernel CalcFFTofRCTensor (Continuation_Function_Module.F90:330-366)
+ *   giem2g_rc_set_anomaly_conductivity  FinalizeRCOperator (:165-196)
+ *   giem2g_rc_recalculate        ReCalculation (:198-239): E and H at the receivers, anomalous part
+ *   giem2g_rc_delete             DeleteRC_OP (:371-380)
+ * Receivers sit on the anomaly's lateral grid: receiver r at cell (ix, iy) is the point
+ * ((ix+1/2) dx + x_shift[r], (iy+1/2) dy + y_shift[r], zrecv[r]).  A receiver depth strictly inside an
+ * anomaly cell is moved to the cell's top border, as PrepareRecvs does; giem2g_rc_receivers reports the
+ * depths used, each receiver's layer and the number of anomaly cells above it.
+ * Fields: E [3][Nz][Ny][Nx] as the IE vectors (Fortran E(Nx,Ny,Nz,3)); Ea, Ha complex(8)
+ * [Ny][Nx][3][Nr] (Fortran Ea(Nr,3,Nx,Ny), the reference's layout).  The total fields add the normal
+ * field of the layered background at the receiver depths (sources_module.F90:26-66).
+ * FP64 throughout.  Nx and Ny powers of two (2*Nx, 2*Ny <= 2048), Nz <= 64, up to 16 layers. */
+void *giem2g_rc_create(GIEM2G_BACKGROUND_TYPE bkg, GIEM2G_ANOMALY_TYPE anomaly, int Nr, const double *zrecv,
+                       const double *x_shift, const double *y_shift);
+int giem2g_rc_receivers(void *rc, double *zrecv, int *recv_layer, int *anom_cell);
+/* bkg.csigb: complex conductivities at the frequency (air first); omega = 2 pi f */
+int giem2g_rc_calc_kernel(void *rc, GIEM2G_BACKGROUND_TYPE bkg, double omega);
+int giem2g_rc_calc_fft_of_kernel(void *rc);
+/* the current tensor (spatial after giem2g_rc_calc_kernel, spectral after giem2g_rc_calc_fft_of_kernel):
+ * complex(8) [2Ny][2Nx][15][Nr][Nz]; lag index ix < Nx is lag ix, ix > Nx is ix - 2Nx, ix = Nx is zero
+ * (same in y); components E xx xy xz yy yz zx zy zz, H xx xy xz yx yz zx zy (const_module.F90:112-130) */
+int giem2g_rc_get_kernel(void *rc, void *G);
+/* csiga complex(8) (Nx,Ny,Nz), x fastest, at the frequency of the kernel (copied) */
+int giem2g_rc_set_anomaly_conductivity(void *rc, const void *csiga);
+int giem2g_rc_recalculate(void *rc, const void *E, void *Ea, void *Ha);
+/* the same with device buffers, on giem2g_rc_get_stream(rc) */
+int giem2g_rc_recalculate_device(void *rc, const void *d_E, void *d_Ea, void *d_Ha);
+void *giem2g_rc_get_stream(void *rc);
+void giem2g_rc_delete(void *rc);
+
 #ifdef __cplusplus
 }
 #endif

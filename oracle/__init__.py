@@ -51,6 +51,7 @@ def lib():
         L.orc_prepare_receivers.argtypes = [vp, ip, vp, vp, vp]
         L.orc_vbt_weights_single.argtypes = [dp, dp, dp, dp, dp, vp, vp]
         L.orc_rc_tensor.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, ip]
+        L.orc_rc_tensor_lags.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, vp, vp, vp, ip]
         L.orc_rc_apply_direct.argtypes = [ip, ip, ip, ip, vp, vp, vp, vp, vp, vp, ip]
         L.orc_rc_apply_fft.argtypes = [ip, ip, ip, ip, vp, vp, vp, vp, vp, vp, ip]
         L.orc_plane_wave_points.argtypes = [vp, ip, ip, vp, vp]
@@ -214,6 +215,17 @@ def rc_tensor(m, rv: Receivers, nthreads: int = 0):
     lib().orc_rc_tensor(ctypes.byref(s), rv.Nr, _p(rv.zrecv), _p(rv.x_shift), _p(rv.y_shift), _p(rv.recv_layer),
                         _p(rv.anom_cell), _p(G), nthreads)
     return G
+
+
+def rc_tensor_lags(m, rv: Receivers, ix, iy, nthreads: int = 0):
+    """Selected lag-plane indices of the receiver tensor: [n, 15, Nr, Nz]."""
+    ix = np.ascontiguousarray(ix, dtype=np.int32)
+    iy = np.ascontiguousarray(iy, dtype=np.int32)
+    out = np.zeros((len(ix), 15, rv.Nr, m.Nz), np.complex128)
+    s, keep = _model_struct(m)
+    lib().orc_rc_tensor_lags(ctypes.byref(s), rv.Nr, _p(rv.zrecv), _p(rv.x_shift), _p(rv.y_shift), _p(rv.recv_layer),
+                             _p(rv.anom_cell), len(ix), _p(ix), _p(iy), _p(out), nthreads)
+    return out
 
 
 def rc_apply(Nx, Ny, Nz, G, csiga, csigb, E, direct: bool = False, nthreads: int = 0):

@@ -1906,6 +1906,47 @@ int orc_rc_tensor(const orc_model *m, int Nr, const double *zrecv, const double 
     return 0;
 }
 
+/* The same for selected lag-plane indices only: out[n][15][Nr][Nz] for (ix[n], iy[n]) */
+int orc_rc_tensor_lags(const orc_model *m, int Nr, const double *zrecv, const double *x_shift, const double *y_shift,
+                       const int *recv_layer, const int *anom_cell, int n, const int *ixs, const int *iys,
+                       double complex *out, int nthreads)
+{
+    int Nx = m->Nx, Ny = m->Ny, Nz = m->Nz;
+    double *depth = (double *)malloc(sizeof(double) * (m->Nl + 1));
+    double complex *k2 = (double complex *)malloc(sizeof(double complex) * (m->Nl + 1));
+    bkg_t b;
+    make_bkg(m, &b, depth, k2);
+    int *L = (int *)malloc(sizeof(int) * (Nz + 1));
+    orc_layer_numbers(m, L);
+    double *dz = (double *)malloc(sizeof(double) * (Nz + 1));
+    for (int i = 1; i <= Nz; i++) dz[i] = m->z[i] - m->z[i - 1];
+    anom_t an = {Nz, L, m->z, dz};
+    vbt_tables *t = (vbt_tables *)malloc(sizeof(vbt_tables));
+    vbt_init(sqrt(m->dx * m->dx + m->dy * m->dy) / 2.0, t);
+    size_t E = (size_t)RC_COMPS * Nr * Nz;
+    memset(out, 0, sizeof(double complex) * E * n);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+#endif
+    for (int k = 0; k < n; k++)
+        for (int r = 0; r < Nr; r++) {
+            int ix = ixs[k], iy = iys[k];
+            if (iy == Ny || ix == Nx) continue;
+            int ly = iy < Ny ? iy : iy - 2 * Ny;
+            int lx = ix < Nx ? ix : ix - 2 * Nx;
+            rc_recv_t rv = {zrecv[r], recv_layer[r], anom_cell[r]};
+            rc_element(t, &b, &an, &rv, x_shift[r], y_shift[r], lx, ly, m->dx, m->dy, out + (size_t)k * E + (size_t)r * Nz,
+                       (size_t)Nr * Nz);
+        }
+    free(t);
+    free(dz);
+    free(L);
+    free(k2);
+    free(depth);
+    return 0;
+}
+
 /* The E and H sums of APPLY_RC_E_OP / APPLY_RC_H_OP (Continuation_Function_Module.F90:382-481) at one
  * point: g = tensor elements [15][Nr][Nz], u = currents [3][Nz]; o[f*3+c][Nr] with f = 0 (E), 1 (H). */
 static void rc_point(int Nr, int Nz, const double complex *g, const double complex *u, double complex *o)

@@ -114,6 +114,9 @@ int orc_vbt_weights_single(double x, double y, double hx, double hy, double rmin
                            double *WT /* [501][6] */, double *lms /* [501] */);
 int orc_rc_tensor(const orc_model *m, int Nr, const double *zrecv, const double *x_shift, const double *y_shift,
                   const int *recv_layer, const int *anom_cell, double complex *G, int nthreads);
+int orc_rc_tensor_lags(const orc_model *m, int Nr, const double *zrecv, const double *x_shift, const double *y_shift,
+                       const int *recv_layer, const int *anom_cell, int n, const int *ix, const int *iy,
+                       double complex *out /* [n][15][Nr][Nz] */, int nthreads);
 int orc_rc_apply_direct(int Nx, int Ny, int Nz, int Nr, const double complex *G, const double complex *csiga,
                         const double complex *csigb, const double complex *E, double complex *Ea,
                         double complex *Ha, int nthreads);

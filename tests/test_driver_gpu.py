@@ -56,3 +56,48 @@ def test_driver_frequency_loop_files_and_warm_start(g2lib, tmp_path):
     # a second run starts every solve from its own solution file: nothing left to iterate
     again = run(path, precision=0, outdir=str(tmp_path), log=None)
     assert all(r["guess"] == "file" and r["stat"] == 1 and r["iterations"] <= 1 for r in again["solves"])
+
+
+def test_driver_receiver_fields(g2lib, orc, tmp_path):
+    """"Recalculate Fields": the P{Y,X}_F files hold the anomalous fields of each solution at the
+    receivers (checked against the oracle's ReCalculation of the same solution with the oracle's own
+    receiver tensor) plus the background's PlaneWave; with "Solve Equation" false the same files come
+    from the saved solutions."""
+    from giem2g_b200.driver import run
+    from giem2g_b200.solution_io import load_receiver_fields, receiver_output_name
+    from giem2g_b200.synthetic import IEModel, csiga_from_sigma
+    path, sig = _write_case(tmp_path, [2.0])
+    inp = json.loads(open(path).read())
+    inp["Recalculate Fields"] = True
+    inp["Recievers"] = [{"depth": 0.0, "xshift": 0.0, "yshift": 0.0},
+                        {"depth": 175.0, "xshift": 10.0, "yshift": -20.0}]   # inside a cell: moved to 150
+    open(path, "w").write(json.dumps(inp))
+    out = run(path, precision=0, outdir=str(tmp_path), log=None)
+    assert out["receivers"]["depth"] == [0.0, 150.0]
+    assert all("recalc_s" in r for r in out["solves"])
+    m = IEModel(16, 16, 8, 100.0, 100.0, np.arange(9) * 50.0, np.array([0.01, 0.001, 0.1]),
+                np.array([500.0, 1500.0]), 2.0)
+    rv = orc.prepare_receivers(m, [0.0, 175.0], [0.0, 10.0], [0.0, -20.0])
+    G = orc.rc_tensor(m, rv)
+    csigb, _ = orc.background_cells(m)
+    csiga = csiga_from_sigma(sig, m.freq)
+    for pol in (EY, EX):
+        E = load_solution(str(tmp_path / solution_name(pol, 2.0)), 16, 16, 8)
+        Ea, Ha = orc.rc_apply(16, 16, 8, G, csiga, csigb, E)
+        F = orc.plane_wave_points(m, pol, rv.zrecv)
+        T = load_receiver_fields(str(tmp_path / receiver_output_name(pol, 2.0)))
+        assert T.shape == (2 * 16 * 16, 28)
+        vals = T[:, 4:].reshape(2, 16, 16, 4, 3, 2)             # [r][y][x][Ea Ha Et Ht][c][re im]
+        got = vals[..., 0] + 1j * vals[..., 1]
+        ref_a = np.stack([np.transpose(Ea, (3, 0, 1, 2)), np.transpose(Ha, (3, 0, 1, 2))], axis=3)
+        ref_t = ref_a + np.stack([F[:, :3], F[:, 3:]], axis=1)[:, None, None]
+        assert np.abs(got[:, :, :, :2] - ref_a).max() < 1e-9 * np.abs(ref_a).max()   # 10 significant digits
+        assert np.abs(got[:, :, :, 2:] - ref_t).max() < 1e-9 * np.abs(ref_t).max()
+    # recalculation only, from the saved solutions
+    first = {pol: (tmp_path / receiver_output_name(pol, 2.0)).read_text() for pol in (EY, EX)}
+    inp["Solve Equation"] = False
+    open(path, "w").write(json.dumps(inp))
+    out2 = run(path, precision=0, outdir=str(tmp_path), log=None)
+    assert [r["solution"] for r in out2["solves"]] == ["file", "file"]
+    for pol in (EY, EX):
+        assert (tmp_path / receiver_output_name(pol, 2.0)).read_text() == first[pol]

@@ -54,3 +54,32 @@ def test_input_json_with_trailing_commas(tmp_path):
     p.write_text('{"Frequencies": [0.1, 1.0,], "FGMRES": {"Tolerance": 1e-8,}, "Recievers": [{"depth": 0},],}')
     d = load_input(str(p))
     assert d["Frequencies"] == [0.1, 1.0] and d["FGMRES"]["Tolerance"] == 1e-8
+
+
+def test_receiver_output_table_layout(tmp_path):
+    from giem2g_b200.solution_io import load_receiver_fields, receiver_output_name, save_receiver_fields
+    assert receiver_output_name(EY, 0.1) == "PY_F00000000000.1000000000.dat"
+    assert receiver_output_name(EX, 10.0) == "PX_F00000000010.0000000000.dat"
+    Ny, Nx, Nr = 2, 3, 2
+    rng = np.random.default_rng(4)
+    F = [rng.standard_normal((Ny, Nx, 3, Nr)) + 1j * rng.standard_normal((Ny, Nx, 3, Nr)) for _ in range(4)]
+    p = tmp_path / "PY.dat"
+    save_receiver_fields(str(p), 50.0, 40.0, [0.0, 120.0], [0.0, 5.0], [0.0, -5.0], 0.1, *F)
+    lines = p.read_text().splitlines()
+    assert lines[0].startswith("%") and len(lines[0]) == 1 + 28 * 20 and lines[0][1:21].strip() == "x_recv"
+    assert all(len(l) == 1 + 28 * 20 and l[0] == " " for l in lines[1:])
+    assert "E+000" in lines[1] or "E-0" in lines[1]
+    T = load_receiver_fields(str(p))
+    assert T.shape == (Nr * Ny * Nx, 28)
+    # receiver outer, then y, then x; x = (ix + 1/2) dx + xshift
+    k = 1 * Ny * Nx + 1 * Nx + 2   # r = 1, iy = 1, ix = 2
+    assert np.allclose(T[k, :4], [2.5 * 50.0 + 5.0, 1.5 * 40.0 - 5.0, 120.0, 0.1])
+    for j, Fa in enumerate(F):
+        got = T[k, 4 + 6 * j: 10 + 6 * j].reshape(3, 2)
+        assert np.allclose(got[:, 0] + 1j * got[:, 1], Fa[1, 2, :, 1], rtol=1e-10)
+
+
+def test_receivers_from_input():
+    from giem2g_b200.solution_io import receivers_from_input
+    z, xs, ys = receivers_from_input({"Recievers": [{"depth": 0, "xshift": 1.5, "yshift": 0}, {"depth": 200.0}]})
+    assert z == [0.0, 200.0] and xs == [1.5, 0.0] and ys == [0.0, 0.0]
