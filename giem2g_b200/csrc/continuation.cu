@@ -256,12 +256,15 @@ G2_D void outfunc2(int i, double s_arg, double cphi, double sphi, double alpha, 
 }
 
 // W layout: [6][npts][NLAM], RC_* order, scaled by lambda and masked (calc_rc_tensor_module.F90:182-222)
-__global__ void __launch_bounds__(256) k_rc_weights(const VbtTab *__restrict__ T, int Nx, int Ny, double dx, double dy,
+__global__ void __launch_bounds__(256, 2) k_rc_weights(const VbtTab *__restrict__ T, int Nx, int Ny, double dx, double dy,
                                                     double xs, double ys, double *W)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *g = reinterpret_cast<double2 *>(smem_raw);  // [VN][6]
-    double *wt = reinterpret_cast<double *>(g + VN * 6);  // [NLAM][6] in RC_* order
+    // [NLAM][6] weights at the top of g: the normalisation reads only g[NFIRST*6 .. (NLAST+1)*6), below it
+    static_assert((NLAST + 1) * 6 * sizeof(double2) <= VN * 6 * sizeof(double2) - NLAM * 6 * sizeof(double),
+                  "weights would overlap the samples still being read");
+    double *wt = reinterpret_cast<double *>(smem_raw + VN * 6 * sizeof(double2) - NLAM * 6 * sizeof(double));
     __shared__ double red[8], w0;
     const int Nx2 = 2 * Nx, Ny2 = 2 * Ny;
     const int pt = blockIdx.x, iy = pt / Nx2, ix = pt - iy * Nx2;
@@ -669,7 +672,7 @@ int rc_calc_kernel(RcOp *op, int Nl, const double2 *csigma, const double *thick,
     double *d_lms = reinterpret_cast<double *>(reinterpret_cast<char *>(d_tab) + offsetof(VbtTab, lms));
     k_rc_basis<<<dim3(NLAM, Nr), 64, 0, st>>>(d_bkg, d_rv, d_lms, d_B);
     RC_TRY2(cudaGetLastError());
-    const size_t smw = sizeof(double2) * VN * 6 + sizeof(double) * NLAM * 6;
+    const size_t smw = sizeof(double2) * VN * 6;  // two blocks per SM
     RC_TRY2(cudaFuncSetAttribute(k_rc_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw));
     const double sc = 1.0 / 4.0 / PI_D;  // s = 1/4/PI (calc_rc_tensor_module.F90:184), G * s (:225-226)
     const int E = (int)op->E();

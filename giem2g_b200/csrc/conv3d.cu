@@ -42,6 +42,32 @@ __global__ void k_im2col3d(const __nv_bfloat16 *__restrict__ x, __nv_bfloat16 *_
     }
 }
 
+// C a multiple of 8 (every layer of the network): one thread per 16-byte vector (8 channels) of a cols
+// row, 32-bit index arithmetic; consecutive threads write consecutive vectors of a row
+__global__ void k_im2col3d_v8(const uint4 *__restrict__ x, uint4 *__restrict__ cols, int D, int H, int W, int C8,
+                              int s, int Do, int Ho, int Wo, int Kp8, int total)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int v = i / Kp8, kv = i - v * Kp8;
+        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+        if (kv < 27 * C8) {
+            const int tap = kv / C8, q = kv - tap * C8;
+            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+            int r = v;
+            const int xo = r % Wo;
+            r /= Wo;
+            const int yo = r % Ho;
+            r /= Ho;
+            const int zo = r % Do;
+            const int n = r / Do;
+            const int zi = zo * s + dz - 1, yi = yo * s + dy - 1, xi = xo * s + dx - 1;
+            if (zi >= 0 && zi < D && yi >= 0 && yi < H && xi >= 0 && xi < W)
+                val = x[(((long long)(n * D + zi) * H + yi) * W + xi) * C8 + q];
+        }
+        cols[i] = val;
+    }
+}
+
 // dx[v][c] = sum over taps of dcols[v'][tap*C + c] for the output voxels v' that read v at that tap
 __global__ void k_col2im3d(const float *__restrict__ dcols, float *__restrict__ dx, int N, int D, int H, int W,
                            int C, int s, int Do, int Ho, int Wo, int Kp)
@@ -95,6 +121,15 @@ int ie_im2col3d(const void *x, void *cols, int N, int D, int H, int W, int C, in
     if (N < 1 || D < 1 || H < 1 || W < 1 || C < 1 || (s != 1 && s != 2) || Kp < 27 * C || (Kp % 8)) return G2_ERR_ARG;
     const int Do = (D - 1) / s + 1, Ho = (H - 1) / s + 1, Wo = (W - 1) / s + 1;
     const long long total = (long long)N * Do * Ho * Wo * Kp;
+    const long long total8 = total / 8;
+    if (C % 8 == 0 && total8 < (1LL << 30) && (reinterpret_cast<uintptr_t>(x) % 16) == 0 &&
+        (reinterpret_cast<uintptr_t>(cols) % 16) == 0) {
+        k_im2col3d_v8<<<grid_for(total8), 256, 0, st>>>(reinterpret_cast<const uint4 *>(x),
+                                                         reinterpret_cast<uint4 *>(cols), D, H, W, C / 8, s, Do, Ho,
+                                                         Wo, Kp / 8, (int)total8);
+        G2_CUDA_CHECK(cudaGetLastError());
+        return G2_OK;
+    }
     k_im2col3d<<<grid_for(total), 256, 0, st>>>(reinterpret_cast<const __nv_bfloat16 *>(x),
                                                 reinterpret_cast<__nv_bfloat16 *>(cols), N, D, H, W, C, s, Do, Ho, Wo, Kp);
     G2_CUDA_CHECK(cudaGetLastError());

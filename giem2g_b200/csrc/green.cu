@@ -242,12 +242,15 @@ G2_D void outfunc(int i, double s_arg, double cphi, double sphi, double alpha, d
 }
 
 // W layout: [6][lags][NLAM] (weight type major), already scaled by lambda and masked
-__global__ void __launch_bounds__(256) k_weights(const VbtTab *__restrict__ T, int Nx, int Ny, double dx, double dy,
+__global__ void __launch_bounds__(256, 2) k_weights(const VbtTab *__restrict__ T, int Nx, int Ny, double dx, double dy,
                                                  double *W)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *g = reinterpret_cast<double2 *>(smem_raw);  // [VN][6]
-    double *wt = reinterpret_cast<double *>(g + VN * 6);  // [NLAM][6] in IE_* order
+    // [NLAM][6] weights at the top of g: the normalisation reads only g[NFIRST*6 .. (NLAST+1)*6), below it
+    static_assert((NLAST + 1) * 6 * sizeof(double2) <= VN * 6 * sizeof(double2) - NLAM * 6 * sizeof(double),
+                  "weights would overlap the samples still being read");
+    double *wt = reinterpret_cast<double *>(smem_raw + VN * 6 * sizeof(double2) - NLAM * 6 * sizeof(double));
     __shared__ double w0[6], red[8][6];
     const int lag = blockIdx.x, lx = lag / Ny, ly = lag - lx * Ny;
     const size_t nlags = (size_t)Nx * Ny;
@@ -399,7 +402,7 @@ int ie_green_tensor(IeOp *op, cudaStream_t st)
     G2_TRY(cudaMalloc(&W, sizeof(double) * 6 * lags * NLAM));
     double *d_lms = reinterpret_cast<double *>(reinterpret_cast<char *>(d_tab) + offsetof(VbtTab, lms));
     k_basis<<<NLAM, 64, 0, st>>>(d_bkg, d_lms, M[0], M[1], M[2], M[3]);
-    const size_t smw = sizeof(double2) * VN * 6 + sizeof(double) * NLAM * 6;
+    const size_t smw = sizeof(double2) * VN * 6;  // two blocks per SM
     G2_TRY(cudaFuncSetAttribute(k_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw));
     k_weights<<<(unsigned)lags, 256, smw, st>>>(d_tab, Nx, Ny, op->dx, op->dy, W);
     G2_TRY(cudaGetLastError());

@@ -27,13 +27,14 @@ def _torch_w(w, cin):
     return w[:, :27 * cin].reshape(cout, 3, 3, 3, cin).permute(0, 4, 1, 2, 3)
 
 
+@pytest.mark.parametrize("C", [12, 16])  # 16: the 16-byte vector im2col (channels a multiple of 8)
 @pytest.mark.parametrize("stride", [1, 2])
-def test_conv3d_layer_vs_cpu(g2lib, stride):
+def test_conv3d_layer_vs_cpu(g2lib, stride, C):
     import torch
     import torch.nn.functional as F
     from giem2g_b200.learned import _kp, conv3d
-    g = torch.Generator().manual_seed(3 + stride)
-    N, D, H, W, C, cout = 2, 4, 6, 8, 12, 16
+    g = torch.Generator().manual_seed(3 + stride + C)
+    N, D, H, W, cout = 2, 4, 6, 8, 16
     x = torch.randn(N, D, H, W, C, generator=g)
     w = torch.zeros(cout, _kp(C))
     w[:, :27 * C] = torch.randn(cout, 27 * C, generator=g) * 0.1

@@ -66,7 +66,7 @@ def test_rc_tensor_matches_oracle(g2lib, orc, shape):
     rc.delete()
 
 
-@pytest.mark.parametrize("shape", [(4, 4, 3), (8, 8, 4)])
+@pytest.mark.parametrize("shape", [(4, 4, 3), (8, 8, 4), (4, 4, 40)])
 def test_rc_recalculate_matches_oracle(g2lib, orc, shape):
     import torch
     m = tiny_model(*shape, freq=3.0)
