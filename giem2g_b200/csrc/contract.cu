@@ -49,6 +49,17 @@ struct CfgT {
     static_assert(MINB * (SMEM + 1024) <= 233472, "MINB CTAs do not fit the SM's shared memory");
 };
 
+// (a.x*b.x + c.x, a.y*b.y + c.y) in one packed FP32 instruction
+G2_D float2 ffma2(float2 a, float2 b, float2 c)
+{
+    union U { float2 f; unsigned long long u; } ua, ub, uc, ud;
+    ua.f = a;
+    ub.f = b;
+    uc.f = c;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(ud.u) : "l"(ua.u), "l"(ub.u), "l"(uc.u));
+    return ud.f;
+}
+
 template <typename R> struct V2;
 template <> struct V2<double> { using T = double2; };
 template <> struct V2<float> { using T = float2; };
@@ -59,11 +70,15 @@ G2_D int sym_idx(int i, int j) { return i <= j ? i + j * (j + 1) / 2 : j + i * (
 // NP > 1: NP vectors share every tensor unit (several right-hand sides of one operator); the spectrum of
 // a unit is [slot][vector][3Nz] and point pt = slot * NP + vector.  SPLIT: each thread computes the 4
 // points of one vector (threads (b, v, s, z)); otherwise each thread holds all 4*NP points.
+// PK (complex64 only): the 3-multiply form with its first two products as one packed fma.rn.f32x2 per
+// term and point, (e.x, e.y) * (u.x, u.y) + (t1, t2), and the third, (e.x + e.y)(u.x + u.y), as a scalar
+// FMA: two instructions per complex multiply-add instead of three; a negative sign uses a negated copy
+// of the tensor element.
 // M4: 4-multiply complex products (two accumulators per output instead of three: 118 registers instead
 // of 142, so three FP64 CTAs fit on an SM, for 12 % more FMAs).  At 128x128x32 it gives 0.395 ms per
 // FP64 apply against 0.388 ms for the 3-multiply tile with a 3-stage ring: occupancy is not what limits
 // the FP64 contraction there, so the tuner keeps the 3-multiply form.
-template <typename R, int NZ, int S, int B, int NSTAGE, int NP, bool SPLIT, int MINB, bool M4>
+template <typename R, int NZ, int S, int B, int NSTAGE, int NP, bool SPLIT, int MINB, bool M4, bool PK>
 __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NTHREADS, MINB)
     k_contract_tma(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
                    long long nbatches, int *err, const int *gate)
@@ -133,8 +148,14 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
         unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
         const C2 *gt = reinterpret_cast<const C2 *>(st);
         const C2 *uh = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);
+        static_assert(!PK || (sizeof(R) == 4 && !M4), "packed pairs are a complex64 3-multiply form");
         constexpr int NA = M4 ? 2 : 3;
         R acc[3][PR][NA];
+        C2 accp[3][PR];  // PK: (t1, t2) of the 3-multiply form
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int p = 0; p < PR; p++) accp[c][p] = C2{R(0), R(0)};
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
@@ -152,6 +173,9 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
             const int si = sym_idx<NZ>(z, j);
             const int a_zj = asw(z, j, NZ, AW), a_jz = asw(j, z, NZ, AW);
             const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[a_zj], gyz[a_zj], gxz[a_jz], gyz[a_jz]};
+            C2 en[8];  // PK: negated copies (only the ones a negative sign uses survive compilation)
+#pragma unroll
+            for (int k = 0; k < 8; k++) en[k] = C2{-e[k].x, -e[k].y};
             C2 u[PR][3];
             R ue[PR][3];
 #pragma unroll
@@ -171,7 +195,10 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
             const R sx = (sl_ & 2) ? R(-1) : R(1);                               \
             const R m = (sl_ & 1) ? R(-1) : R(1);                                \
             const R sg = (SGN);                                                  \
-            if constexpr (M4) {                                                  \
+            if constexpr (PK) {                                                  \
+                accp[C][p] = ffma2(sg < R(0) ? en[K] : e[K], u[p][IN], accp[C][p]); \
+                acc[C][p][NA - 1] = fma(sg * es_, ue[p][IN], acc[C][p][NA - 1]); \
+            } else if constexpr (M4) {                                           \
                 acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);       \
                 acc[C][p][0] = fma(-sg * e[K].y, u[p][IN].y, acc[C][p][0]);      \
                 acc[C][p][1] = fma(sg * e[K].x, u[p][IN].y, acc[C][p][1]);       \
@@ -205,7 +232,11 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 C2 o;
-                if constexpr (M4) {
+                if constexpr (PK) {
+                    const R t1 = accp[c][p].x, t2 = accp[c][p].y, t3 = acc[c][p][NA - 1];
+                    o.x = t1 - t2;
+                    o.y = t3 - t1 - t2;
+                } else if constexpr (M4) {
                     o.x = acc[c][p][0];
                     o.y = acc[c][p][1];
                 } else {
@@ -271,16 +302,6 @@ struct CfgW {
     static_assert(SMEM <= 232448, "exceeds the 227 KB dynamic shared memory of one CTA");
     static_assert(MINB * (SMEM + 1024) <= 233472, "MINB CTAs do not fit the SM's shared memory");
 };
-
-G2_D float2 ffma2(float2 a, float2 b, float2 c)
-{
-    union U { float2 f; unsigned long long u; } ua, ub, uc, ud;
-    ua.f = a;
-    ub.f = b;
-    uc.f = c;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(ud.u) : "l"(ua.u), "l"(ub.u), "l"(uc.u));
-    return ud.f;
-}
 
 template <int NZ, int S, int B, int NSTAGE, int NP, int MINB>
 __global__ void __launch_bounds__(CfgW<NZ, S, B, NSTAGE, NP, MINB>::NTHREADS, MINB)
@@ -496,11 +517,12 @@ int launch_w32(const float2 *G, float2 *Uhat, int Nx, int Ny, int *err, int nsm,
 }
 
 // MINB CTAs per SM: their compute, reduction and barrier phases overlap one another
-template <typename R, int NZ, int S, int B, int NSTAGE, int NP = 1, bool SPLIT = false, int MINB = 1, bool M4 = false>
+template <typename R, int NZ, int S, int B, int NSTAGE, int NP = 1, bool SPLIT = false, int MINB = 1, bool M4 = false,
+          bool PK = false>
 int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
     using Cfg = CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>;
-    auto kern = k_contract_tma<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB, M4>;
+    auto kern = k_contract_tma<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB, M4, PK>;
     nsm *= MINB;
     static bool attr = false;
     if (!attr) {
@@ -535,7 +557,7 @@ int sm_count()
 int ie_contract_variants(int precision, int Nz)
 {
     if (precision == 0) return Nz == 32 ? 5 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
-    return Nz == 32 ? 12 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    return Nz == 32 ? 14 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
@@ -581,6 +603,8 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         case 9: return launch_cfg<float, 32, 2, 1, 1, 1, false, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 10: return launch_cfg<float, 32, 2, 1, 2, 1, false, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 11: return launch_w32<32, 4, 1, 2, 1, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 12: return launch_cfg<float, 32, 4, 1, 2, 1, false, 3, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 13: return launch_cfg<float, 32, 4, 1, 3, 1, false, 2, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         default: return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
         }
     case 48:
@@ -594,7 +618,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 8 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 9 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -616,6 +640,7 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         if (v == 5) return launch_cfg<float, 32, 4, 1, 2, 2, false, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 6) return launch_cfg<float, 32, 2, 1, 1, 2, true, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 7) return launch_w32<32, 4, 1, 2, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 8) return launch_cfg<float, 32, 4, 1, 2, 2, false, 2, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 32, 4, 2, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
