@@ -80,7 +80,8 @@ EXPORTED_SYMBOLS = [
     "giem2g_set_kernel_timing", "giem2g_last_contract_ms",
     "giem2g_rc_create", "giem2g_rc_receivers", "giem2g_rc_calc_kernel", "giem2g_rc_calc_fft_of_kernel",
     "giem2g_rc_get_kernel", "giem2g_rc_set_anomaly_conductivity", "giem2g_rc_recalculate",
-    "giem2g_rc_recalculate_device", "giem2g_rc_get_stream", "giem2g_rc_delete",
+    "giem2g_rc_recalculate_device", "giem2g_rc_get_stream", "giem2g_rc_delete", "giem2g_set_precision",
+    "giem2g_set_preconditioner", "giem2g_preconditioner_calls", "giem2g_apply_preconditioner",
 ]
 
 
@@ -147,6 +148,11 @@ def lib():
     L.giem2g_col2im3d_f32.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
     L.giem2g_set_outer_preconditioner.argtypes = [vp, ip, PRECOND_FN, vp]
     L.giem2g_set_fft_lines.argtypes = [vp, ip]
+    L.giem2g_set_precision.argtypes = [vp, ip]
+    L.giem2g_set_preconditioner.argtypes = [vp, ip, ctypes.c_char_p]
+    L.giem2g_preconditioner_calls.argtypes = [vp]
+    L.giem2g_preconditioner_calls.restype = ctypes.c_longlong
+    L.giem2g_apply_preconditioner.argtypes = [vp, vp, vp]
     L.giem2g_set_kernel_timing.argtypes = [vp, ip]
     L.giem2g_last_contract_ms.argtypes = [vp]
     L.giem2g_last_contract_ms.restype = dp
@@ -302,6 +308,26 @@ class IEOperator:
 
     def set_contract_variant(self, precision: int, variant: int):
         _check(lib().giem2g_set_contract_variant(self.handle, precision, variant), "set_contract_variant")
+
+    def set_precision(self, mode: int):
+        """giem2g_set_precision: 1 makes apply_precond compute in complex64 and is the precision of
+        solves called with precision=-1."""
+        _check(lib().giem2g_set_precision(self.handle, int(mode)), "set_precision")
+
+    def set_preconditioner(self, kind: int, weights_path: str | None = None):
+        """giem2g_set_preconditioner: the learned U-Net evaluated inside the library (kind 1: warm start of the
+        inner GMRES, 2: replaces it, 0: off).  Default weights: weights/unet3d_c4.npz next to this module."""
+        if weights_path is None and kind:
+            weights_path = os.path.join(_HERE, "weights", "unet3d_c4.npz")
+        _check(lib().giem2g_set_preconditioner(self.handle, int(kind), weights_path.encode() if weights_path else None),
+               "set_preconditioner")
+
+    def apply_preconditioner(self, d_v: int, d_z: int):
+        """giem2g_apply_preconditioner: d_z = the registered network's guess of A^-1 v (device pointers)."""
+        _check(lib().giem2g_apply_preconditioner(self.handle, d_v, d_z), "apply_preconditioner")
+
+    def preconditioner_calls(self) -> int:
+        return int(lib().giem2g_preconditioner_calls(self.handle))
 
     def set_fft_lines(self, lines: int):
         _check(lib().giem2g_set_fft_lines(self.handle, lines), "set_fft_lines")

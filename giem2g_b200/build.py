@@ -47,7 +47,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         list(ex.map(run, jobs))
     objs = [os.path.join(OBJ, os.path.basename(c)[:-3] + ".o") for c in cus]
     if force or jobs or _deps_newer(LIB, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)

@@ -14,6 +14,7 @@
 // (kx-pair q, ky-pair r, slot s) <-> (kx,ky): kx = q (s&2==0) or 2Nx-q, with q=0,s&2 the x-Nyquist;
 // ky = r (s&1==0) or 2Ny-r, with r=0,s&1 the y-Nyquist.  Nyquist outputs are zero as in the
 // reference (FinalTransposeRepack / DistributedFourierYRepack drop them).
+#include <algorithm>
 #include <type_traits>
 #include "common.cuh"
 #include "fft4.cuh"
@@ -458,6 +459,38 @@ int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_
 {
     return ie_apply_device<double>(op, d_in, d_out, st, gate);
 }
+namespace {
+__global__ void k_c128_to_c64(const double2 *__restrict__ a, float2 *__restrict__ b, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+__global__ void k_c64_to_c128(const float2 *__restrict__ a, double2 *__restrict__ b, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = make_double2((double)a[i].x, (double)a[i].y);
+}
+}  // namespace
+
+// The reference-facing apply in the operator's precision mode 1: complex128 in and out, complex64 inside.
+int ie_apply_host_mixed(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st)
+{
+    const long long n = (long long)op->nvec();
+    if (!op->d_vin32) {
+        G2_CUDA_CHECK(cudaMalloc(&op->d_vin32, n * sizeof(float2)));
+        G2_CUDA_CHECK(cudaMalloc(&op->d_vout32, n * sizeof(float2)));
+    }
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_c128_to_c64<<<blocks, 256, 0, st>>>(d_in, op->d_vin32, n);
+    G2_CUDA_CHECK(cudaGetLastError());
+    int rc = ie_apply_device32(op, op->d_vin32, op->d_vout32, st);
+    if (rc) return rc;
+    k_c64_to_c128<<<blocks, 256, 0, st>>>(op->d_vout32, d_out, n);
+    G2_CUDA_CHECK(cudaGetLastError());
+    g2_count_launches(2);
+    return G2_OK;
+}
+
 int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, const int *gate)
 {
     return ie_apply_device<float>(op, d_in, d_out, st, gate);
@@ -516,6 +549,9 @@ static int make_tw(int L, double2 **d64, float2 **d32)
     G2_CUDA_CHECK(cudaMalloc(d32, sizeof(float2) * L));
     G2_CUDA_CHECK(cudaMemcpy(*d64, h64.data(), sizeof(double2) * L, cudaMemcpyHostToDevice));
     G2_CUDA_CHECK(cudaMemcpy(*d32, h32.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+    // a pageable cudaMemcpy may return before its DMA lands, and the operator's non-blocking stream is
+    // not ordered after the legacy stream: wait for it here
+    G2_CUDA_CHECK(cudaStreamSynchronize(cudaStreamLegacy));
     return G2_OK;
 }
 

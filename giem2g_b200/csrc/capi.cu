@@ -147,7 +147,8 @@ void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data
     int rc = ie_make_twiddles(op);
     if (!rc) rc = ie_alloc_scratch(op);
     if (!rc && !op->d_err) {
-        if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess)
+        if (cudaMalloc(&op->d_err, sizeof(int)) != cudaSuccess || cudaMemset(op->d_err, 0, sizeof(int)) != cudaSuccess ||
+            cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess)
             rc = G2_ERR_NOMEM;
     }
     if (!rc && !op->d_csiga && cudaMalloc(&op->d_csiga, op->cells() * sizeof(double2)) != cudaSuccess) rc = G2_ERR_NOMEM;
@@ -233,7 +234,10 @@ int giem2g_set_ie_kernel_spatial(void *ie, const void *symm, const void *asym)
         std::memcpy(&h[u * T], s + u * 4 * P, sizeof(double2) * 4 * P);
         std::memcpy(&h[u * T + 4 * P], a + u * 2 * Nz * Nz, sizeof(double2) * 2 * Nz * Nz);
     }
-    if (cudaMemcpy(op->d_spatial, h.data(), U * T * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+    // stream-ordered: the transform that follows runs on the operator's (non-blocking) stream
+    if (cudaMemcpyAsync(op->d_spatial, h.data(), U * T * sizeof(double2), cudaMemcpyHostToDevice, op->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(op->stream) != cudaSuccess)
         return fail(G2_ERR_CUDA, "giem2g_set_ie_kernel_spatial: copy failed");
     op->have_spatial = true;
     op->have_spectral = false;
@@ -245,7 +249,8 @@ static int get_units(IeOp *op, const double2 *d, void *symm, void *asym, int W =
     const int P = op->P(), Nz = op->Nz, T = op->Tunit();
     const size_t U = op->units();
     std::vector<double2> h(U * T);
-    if (cudaMemcpy(h.data(), d, U * T * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpyAsync(h.data(), d, U * T * sizeof(double2), cudaMemcpyDeviceToHost, op->stream) != cudaSuccess ||
+        cudaStreamSynchronize(op->stream) != cudaSuccess)
         return fail(G2_ERR_CUDA, "tensor download failed");
     double2 *s = reinterpret_cast<double2 *>(symm), *a = reinterpret_cast<double2 *>(asym);
     for (size_t u = 0; u < U; u++) {
@@ -287,7 +292,9 @@ void giem2g_set_anomaly_conductivity(void *ie, void *csiga)
     IeOp *op = resolve(ie);
     if (!op || !op->d_csiga) { fail(G2_ERR_STATE, "giem2g_set_anomaly_conductivity: operator not prepared"); return; }
     if (!csiga) { fail(G2_ERR_ARG, "giem2g_set_anomaly_conductivity: csiga is NULL"); return; }
-    if (cudaMemcpy(op->d_csiga, csiga, op->cells() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (cudaMemcpyAsync(op->d_csiga, csiga, op->cells() * sizeof(double2), cudaMemcpyHostToDevice, op->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(op->stream) != cudaSuccess) {
         fail(G2_ERR_CUDA, "giem2g_set_anomaly_conductivity: copy failed");
         return;
     }
@@ -367,7 +374,16 @@ void giem2g_apply_ie_operator(void *ie, void *in, void *out)
     if (check_ready(op, "giem2g_apply_ie_operator")) return;
     const size_t nb = op->nvec() * sizeof(double2);
     cudaMemcpyAsync(op->d_vin, in, nb, cudaMemcpyHostToDevice, op->stream);
-    int rc = giem2g_apply_ie_operator_device(op, op->d_vin, op->d_vout, 0);
+    int rc;
+    if (op->precision_mode == 1) {  // giem2g_set_precision(ie, 1)
+        cudaEventRecord(op->ev0, op->stream);
+        rc = ie_apply_host_mixed(op, op->d_vin, op->d_vout, op->stream);
+        cudaEventRecord(op->ev1, op->stream);
+        op->mult_num++;
+        if (rc) { fail(rc, "giem2g_apply_ie_operator: %s", giem2g_last_error()); return; }
+    } else {
+        rc = giem2g_apply_ie_operator_device(op, op->d_vin, op->d_vout, 0);
+    }
     if (rc) return;
     cudaMemcpyAsync(out, op->d_vout, nb, cudaMemcpyDeviceToHost, op->stream);
     if (cudaStreamSynchronize(op->stream) != cudaSuccess) { fail(G2_ERR_CUDA, "giem2g_apply_ie_operator: %s", cudaGetErrorString(cudaGetLastError())); return; }
@@ -376,6 +392,44 @@ void giem2g_apply_ie_operator(void *ie, void *in, void *out)
     cudaEventElapsedTime(&ms, op->ev0, op->ev1);
     op->apply_seconds += ms * 1e-3;
     set_status(0);
+}
+
+int giem2g_set_preconditioner(void *ie, int kind, const char *weights_path)
+{
+    IeOp *op = resolve(ie);
+    if (!op) return fail(G2_ERR_STATE, "giem2g_set_preconditioner: no operator");
+    if (kind < 0 || kind > 2) return fail(G2_ERR_ARG, "giem2g_set_preconditioner: kind must be 0, 1 or 2");
+    const int rc = ie_set_learned_preconditioner(op, kind, weights_path);
+    if (rc) return set_status(rc);
+    return set_status(0);
+}
+
+int giem2g_apply_preconditioner(void *ie, const void *d_v, void *d_z)
+{
+    IeOp *op = resolve(ie);
+    if (!op || !d_v || !d_z) return fail(G2_ERR_ARG, "giem2g_apply_preconditioner: null argument");
+    return set_status(ie_learned_apply(op, reinterpret_cast<const double2 *>(d_v), reinterpret_cast<double2 *>(d_z)));
+}
+
+long long giem2g_preconditioner_calls(void *ie)
+{
+    IeOp *op = resolve(ie);
+    return op ? ie_learned_calls(op) : 0;
+}
+
+int giem2g_set_precision(void *ie, int mode)
+{
+    IeOp *op = resolve(ie);
+    if (!op) return fail(G2_ERR_STATE, "giem2g_set_precision: no operator");
+    if (mode != 0 && mode != 1) return fail(G2_ERR_ARG, "giem2g_set_precision: mode must be 0 or 1");
+    op->precision_mode = mode;
+    return set_status(0);
+}
+
+static GIEM2G_FGMRES_CTL resolve_precision(const IeOp *op, GIEM2G_FGMRES_CTL ctl)
+{
+    if (ctl.precision < 0) ctl.precision = op->precision_mode;
+    return ctl;
 }
 
 int giem2g_set_contract_variant(void *ie, int precision, int variant)
@@ -440,7 +494,7 @@ int giem2g_solve_device(void *ie, const void *d_Ebkg, void *d_Esol, const void *
     if (rc) return rc;
     if (!d_Ebkg || !d_Esol || !info) return fail(G2_ERR_ARG, "giem2g_solve_device: NULL argument");
     rc = krylov_solve_device(op, reinterpret_cast<const double2 *>(d_Ebkg), reinterpret_cast<double2 *>(d_Esol),
-                             reinterpret_cast<const double2 *>(d_E0), ctl, info);
+                             reinterpret_cast<const double2 *>(d_E0), resolve_precision(op, ctl), info);
     if (rc) return fail(rc, "giem2g_solve_device: %s", giem2g_last_error());
     return set_status(0);
 }
@@ -460,7 +514,7 @@ int giem2g_solve(void *ie, const void *E_bkg, void *Esol, const void *E0, GIEM2G
         if (cudaMalloc(&d_e0, nb) != cudaSuccess) return fail(G2_ERR_NOMEM, "giem2g_solve: cudaMalloc failed");
         cudaMemcpyAsync(d_e0, E0, nb, cudaMemcpyHostToDevice, op->stream);
     }
-    rc = krylov_solve_device(op, op->d_vin, op->d_vout, d_e0, ctl, info);
+    rc = krylov_solve_device(op, op->d_vin, op->d_vout, d_e0, resolve_precision(op, ctl), info);
     if (d_e0) cudaFree(d_e0);
     if (rc) return fail(rc, "giem2g_solve: %s", giem2g_last_error());
     if (cudaMemcpyAsync(Esol, op->d_vout, nb, cudaMemcpyDeviceToHost, op->stream) != cudaSuccess ||
@@ -478,6 +532,7 @@ void *giem2g_batch_create(void *const *ies, int n, GIEM2G_FGMRES_CTL ctl)
         if (check_ready(ops[i], "giem2g_batch_create")) return nullptr;
     }
     void *b = nullptr;
+    if (ctl.precision < 0) ctl.precision = ops[0]->precision_mode;
     const int rc = batch_create(ops.data(), n, ctl.fgmres_buf, ctl.gmres_buf, ctl.precision, &b);
     if (rc) { fail(rc, "giem2g_batch_create: %s", giem2g_last_error()); return nullptr; }
     set_status(0);
@@ -584,7 +639,8 @@ int giem2g_gemm_bf16_tn(const void *A, const void *B, float *C, int M, int N, in
 {
     static int *own_err = nullptr;
     if (!d_err) {
-        if (!own_err && (cudaMalloc(&own_err, sizeof(int)) != cudaSuccess || cudaMemset(own_err, 0, sizeof(int)) != cudaSuccess))
+        if (!own_err && (cudaMalloc(&own_err, sizeof(int)) != cudaSuccess || cudaMemset(own_err, 0, sizeof(int)) != cudaSuccess ||
+                         cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess))
             return fail(G2_ERR_NOMEM, "giem2g_gemm_bf16_tn: error word");
         d_err = own_err;
     }
@@ -821,11 +877,12 @@ void giem2g_delete_ie_operator(void *ie)
     IeOp *op = resolve(ie);
     if (!op) return;
     if (op->stream) cudaStreamSynchronize(op->stream);
+    ie_free_learned(op);
     krylov_free(op);
     void *ptrs[] = {op->d_spatial, op->d_tensor64, op->d_tensor32, op->d_csiga, op->d_gsig64, op->d_asig64,
                     op->d_gsig32, op->d_asig32, op->d_post64, op->d_post32, op->d_twx64, op->d_twy64,
                     op->d_twx32, op->d_twy32, op->scratch.U1, op->scratch.Uhat, op->pair_scratch.U1,
-                    op->pair_scratch.Uhat, op->d_vin, op->d_vout, op->d_err};
+                    op->pair_scratch.Uhat, op->d_vin, op->d_vout, op->d_err, op->d_vin32, op->d_vout32};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (op->ev0) cudaEventDestroy(op->ev0);
@@ -844,10 +901,12 @@ int ie_check_device_error(IeOp *op)
 {
     int h = 0;
     if (!op->d_err) return 0;
-    if (cudaMemcpy(&h, op->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    if ((op->stream && cudaStreamSynchronize(op->stream) != cudaSuccess) ||
+        cudaMemcpy(&h, op->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
         return fail(G2_ERR_CUDA, "error-word read failed");
     if (h) {
         cudaMemset(op->d_err, 0, sizeof(int));
+        cudaStreamSynchronize(cudaStreamLegacy);
         return fail(G2_ERR_NUMERIC, "device wait limit reached (code %d)", h);
     }
     return 0;

@@ -538,12 +538,16 @@ RcOp *rc_create(int Nx, int Ny, int Nz, double dx, double dy, const double *z, i
     if (ok) {
         make_twiddles(tw, 2 * Nx);
         ok = cudaMalloc(&op->d_twx, tw.size() * sizeof(double2)) == cudaSuccess &&
-             cudaMemcpy(op->d_twx, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess;
+             cudaMemcpyAsync(op->d_twx, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, op->stream) ==
+                 cudaSuccess &&
+             cudaStreamSynchronize(op->stream) == cudaSuccess;
     }
     if (ok) {
         make_twiddles(tw, 2 * Ny);
         ok = cudaMalloc(&op->d_twy, tw.size() * sizeof(double2)) == cudaSuccess &&
-             cudaMemcpy(op->d_twy, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice) == cudaSuccess;
+             cudaMemcpyAsync(op->d_twy, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice, op->stream) ==
+                 cudaSuccess &&
+             cudaStreamSynchronize(op->stream) == cudaSuccess;
     }
     if (!ok) {
         g2_set_error_msg("rc_create: device allocation failed");

@@ -46,6 +46,7 @@ struct IeOp {
     // host staging for the reference-facing (host-pointer) apply
     double2 *h_stage_in = nullptr, *h_stage_out = nullptr;
     double2 *d_vin = nullptr, *d_vout = nullptr;
+    float2 *d_vin32 = nullptr, *d_vout32 = nullptr;  // complex64 copies for the mode-1 host apply
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // events around the contraction launch of eager device applies (giem2g_set_kernel_timing)
@@ -61,6 +62,7 @@ struct IeOp {
     int precond_mode = 0;
     int (*precond_fn)(void *, const void *, void *, long long, void *) = nullptr;
     void *precond_user = nullptr;
+    void *learned = nullptr;           // network of giem2g_set_preconditioner (learned_net.cu), owned
     // counters (Integral_Equation_Module.F90:44-56)
     long long mult_num = 0;
     double apply_seconds = 0;
@@ -78,6 +80,8 @@ struct IeOp {
 // solver to skip Arnoldi steps after convergence without a host round trip)
 int ie_apply_device64(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, const int *gate = nullptr);
 int ie_apply_device32(IeOp *op, const float2 *d_in, float2 *d_out, cudaStream_t st, const int *gate = nullptr);
+// complex128 in/out, complex64 apply inside (giem2g_set_precision mode 1)
+int ie_apply_host_mixed(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st);
 // The same apply over caller-given scratch (U1: first n_u1 elements, Uhat: the rest).
 size_t ie_apply_scratch_elems(const IeOp *op, size_t *n_u1);
 int ie_apply_device64_scratch(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, double2 *U1,
@@ -106,6 +110,12 @@ int ie_gemm_bf16_tn(const void *A, const void *B, float *C, int M, int N, int K,
 int ie_alloc_scratch(IeOp *op);
 int ie_make_twiddles(IeOp *op);
 int ie_kernel_launch_count_apply();
+
+// learned_net.cu: the U-Net outer preconditioner (kind 0 off, 1 warm start, 2 replace)
+int ie_set_learned_preconditioner(IeOp *op, int kind, const char *weights_path);
+long long ie_learned_calls(const IeOp *op);
+int ie_learned_apply(IeOp *op, const double2 *d_v, double2 *d_z);
+void ie_free_learned(IeOp *op);
 
 // green.cu: spatial Green's tensor (FP64) into op->d_spatial
 int ie_green_tensor(IeOp *op, cudaStream_t st);

@@ -530,6 +530,8 @@ static int alloc_level(Level &L, int m)
     G2_CUDA_CHECK(cudaMemset(L.counter, 0, sizeof(unsigned)));
     G2_CUDA_CHECK(cudaMemset(L.flags, 0, sizeof(int) * F_NFLAGS));
     G2_CUDA_CHECK(cudaMemset(L.scal, 0, sizeof(double) * S_NSCAL));
+    // the solver's kernels run on non-blocking streams, which are not ordered after the legacy stream
+    G2_CUDA_CHECK(cudaStreamSynchronize(cudaStreamLegacy));
     return G2_OK;
 }
 static void free_level(Level &L)
@@ -1423,7 +1425,7 @@ int batch_solve_device(void *h, const double2 *const *d_Ebkg, double2 *const *d_
 {
     BatchWork *b = reinterpret_cast<BatchWork *>(h);
     if (!b) return G2_ERR_STATE;
-    if (ctl.fgmres_buf != b->mo || ctl.gmres_buf != b->mi || ctl.precision != b->precision) {
+    if (ctl.fgmres_buf != b->mo || ctl.gmres_buf != b->mi || (ctl.precision >= 0 && ctl.precision != b->precision)) {
         g2_set_error_msg("batched solve: buffer sizes or precision differ from the batch's");
         return G2_ERR_ARG;
     }

@@ -130,8 +130,14 @@ typedef struct {
     int fgmres_maxit;    /* MaxRestart */
     int gmres_buf;       /* InnerBufferSize */
     int fgmres_buf;      /* OuterBufferSize */
-    int precision;       /* 0 plain FP64; 1 mixed: complex64 inner GMRES, FP64 outer */
+    int precision;       /* 0 plain FP64; 1 mixed: complex64 inner GMRES, FP64 outer;
+                            -1: the operator's mode (giem2g_set_precision) */
 } GIEM2G_FGMRES_CTL;
+
+/* The operator's precision mode (default 0).  Mode 1 makes the reference-facing apply
+ * giem2g_apply_ie_operator compute in complex64 (its vectors stay complex(8)) and is the precision of
+ * solves and batches whose control block says -1.  No counterpart in the reference (FP64 only). */
+int giem2g_set_precision(void *ie, int mode);
 
 /* RESULT_INFO (GFGMRES/fgmres_interfaces.F90:34-39) + counters */
 typedef struct {
@@ -164,6 +170,17 @@ int giem2g_get_misfit_history(void *ie, double *out, int max_len);
  * the solve.  Single-instance solves only (giem2g_solve, giem2g_solve_device). */
 typedef int (*giem2g_precond_fn)(void *user, const void *d_v, void *d_z, long long n, void *stream);
 int giem2g_set_outer_preconditioner(void *ie, int mode, giem2g_precond_fn fn, void *user);
+/* The learned preconditioner in that slot without a host-side network: kind 0 = plain inner GMRES
+ * (removes it), 1 = the network's guess starts the inner GMRES cycle, 2 = the guess replaces the inner
+ * cycle (with the fallback rule above).  weights_path: the .npz of giem2g_b200/weights (float32 [Cout][Kp]
+ * matrices of the 12 convolutions); the network reads log10 of the operator's anomaly conductivity (set
+ * it first) and its frequency.  Nx, Ny, Nz must be multiples of 8.  No counterpart in the reference. */
+int giem2g_set_preconditioner(void *ie, int kind, const char *weights_path);
+/* network evaluations since giem2g_set_preconditioner */
+long long giem2g_preconditioner_calls(void *ie);
+/* the registered network once, outside a solve: d_z = d_v + rms(d_v) * net(d_v) (complex128, device,
+ * 3*Nx*Ny*Nz elements, on the operator's stream; synchronises) */
+int giem2g_apply_preconditioner(void *ie, const void *d_v, void *d_z);
 
 /* ---- batched solves -----------------------------------------------------------
  * The reference solves one (frequency, polarisation) after another (giem2g.F90:336-373).  A batch

@@ -108,3 +108,41 @@ def test_complex64_specialised_and_generic_contraction(g2lib, orc, shape, monkey
         op.check_device_error()
         assert rel(do64.cpu().numpy().reshape(v.shape), out_o) < TOL64
         op.delete()
+
+
+def test_precision_mode_of_the_host_apply_and_solve(g2lib, orc):
+    """giem2g_set_precision: mode 1 makes the reference-facing apply run in complex64 (within the complex64
+    tolerance of the oracle, and not the FP64 result), and solves with precision -1 follow the mode."""
+    m = tiny_model(8, 8, 8)
+    symm, asym = random_spatial_tensor(m, seed=5)
+    sig = random_sigma(m, 6)
+    op, csiga, csigb, sqsigb = _setup(g2lib, orc, m, symm, asym, sig)
+    sh, ah = orc.tensor_spectrum(m.Nx, m.Ny, m.Nz, symm, asym)
+    v = random_vec(m, 7)
+    ref = orc.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v)
+    y64 = op.apply_precond(v)
+    op.set_precision(1)
+    y32 = op.apply_precond(v)
+    assert rel(y64, ref) < TOL64
+    assert rel(y32, ref) < TOL32 and rel(y32, ref) > 1e-10
+    op.set_precision(0)
+    assert rel(op.apply_precond(v), ref) < TOL64
+    with pytest.raises(g2lib.Giem2gError):
+        op.set_precision(2)
+    op.delete()
+    # solves: precision -1 takes the operator's mode
+    mb, sgb = config_small_block()
+    op = g2lib.IEOperator.from_model(mb)
+    op.calc_ie_kernel(mb.csigma, mb.thick, mb.omega)
+    op.calc_fft_of_ie_kernel()
+    op.set_anomaly_sigma(sgb, mb.freq)
+    from giem2g_b200.sources import plane_wave_integral
+    E0 = plane_wave_integral(mb, 1)
+    _, i1 = op.solve_equation(E0, tol=1e-6, precision=1)
+    op.set_precision(1)
+    _, im = op.solve_equation(E0, tol=1e-6, precision=-1)
+    assert im.applies_fp32 > 0 and im.iterations == i1.iterations and im.applies_fp32 == i1.applies_fp32
+    op.set_precision(0)
+    _, i0 = op.solve_equation(E0, tol=1e-6, precision=-1)
+    assert i0.applies_fp32 == 0
+    op.delete()

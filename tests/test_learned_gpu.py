@@ -202,3 +202,35 @@ def test_trained_network_gain(g2lib):
     assert warm.iterations <= plain.iterations + 1
     assert only.precond_steps <= 2 and only.iterations <= plain.iterations + 3
     op.delete()
+
+
+def test_library_network_matches_python_hook(g2lib):
+    """giem2g_set_preconditioner evaluates the committed network inside the library (weights read from the
+    .npz, the same kernels and BF16 roundings): the solves take the same outer iterations and misfit history
+    as with the Python hook, in both modes, and kind 0 restores the plain solve."""
+    import torch
+    from giem2g_b200.learned import WEIGHTS, LearnedPreconditioner, UNet3D
+    m, sig, op = _c4_op(g2lib, 904)
+    b = torch.from_numpy(np.ascontiguousarray(plane_wave_integral(m, 1)).ravel()).cuda()
+    y_py, y_lib, y0 = torch.empty_like(b), torch.empty_like(b), torch.empty_like(b)
+    plain = op.solve_device(b.data_ptr(), y0.data_ptr(), None, tol=1e-6, precision=1)
+    pre = LearnedPreconditioner(UNet3D.from_file(WEIGHTS), m, sig)
+    for mode in (1, 2):
+        pre.attach(op, mode)
+        i_py = op.solve_device(b.data_ptr(), y_py.data_ptr(), None, tol=1e-6, precision=1)
+        op.set_outer_preconditioner(0)
+        op.set_preconditioner(mode, WEIGHTS)
+        i_lib = op.solve_device(b.data_ptr(), y_lib.data_ptr(), None, tol=1e-6, precision=1)
+        torch.cuda.synchronize()
+        assert i_lib.stat == i_py.stat == 1
+        assert i_lib.iterations == i_py.iterations and i_lib.precond_steps == i_py.precond_steps
+        assert np.allclose(i_lib.misfits, i_py.misfits, rtol=1e-3, atol=0)
+        assert float((y_lib - y_py).norm() / y_py.norm()) < 1e-5
+        assert op.preconditioner_calls() >= i_lib.precond_steps >= 1
+    op.set_preconditioner(0)
+    again = op.solve_device(b.data_ptr(), y_lib.data_ptr(), None, tol=1e-6, precision=1)
+    torch.cuda.synchronize()
+    assert again.iterations == plain.iterations and float((y_lib - y0).norm() / y0.norm()) < 1e-12
+    with pytest.raises(g2lib.Giem2gError):
+        op.set_preconditioner(1, "/nonexistent/weights.npz")
+    op.delete()
