@@ -1,0 +1,80 @@
+"""The benchmark's own workload (128x128x32 cells of 50x50x25 m, seeded GRF conductivity, 3-layer
+background, 0.1 Hz) against the oracle at full size: the Green's tensor at every lag, its spectrum, the apply
+in both precisions, and the solves (the GPU solution put back through the oracle's apply).
+
+Tolerances as on the small grids: tensor 1e-10 relative (cross-layer xx/xy/yy entries bounded at 5 % of the
+block, as in test_green_gpu.py: the anomaly crosses the 500 m interface), spectrum and FP64 apply 1e-12,
+complex64 apply 2e-5; the recomputed relative residual of a solve stays within 1.5x the solver's tolerance.
+"""
+import numpy as np
+import pytest
+
+from giem2g_b200.sources import plane_wave_integral
+from giem2g_b200.synthetic import config_c2, csiga_from_sigma
+from tests.helpers import random_vec, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c2(g2lib):
+    m, sig = config_c2(seed=2024)
+    op = g2lib.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    S_g, A_g = op.get_ie_kernel_spatial()
+    op.calc_fft_of_ie_kernel()
+    op.set_anomaly_sigma(sig, m.freq)
+    yield m, sig, op, S_g, A_g
+    op.delete()
+
+
+def test_c2_tensor_matches_oracle(c2, orc):
+    from tests.test_green_gpu import _cross_layer_mask
+    m, sig, op, S_g, A_g = c2
+    S_o, A_o = orc.green_tensor(m)
+    cross = _cross_layer_mask(orc.layer_numbers(m), m.Nz)
+    assert cross.any()  # the anomaly crosses a layer interface
+    assert rel(S_g[:, :, 3], S_o[:, :, 3]) < 1e-10
+    for c in range(2):
+        assert rel(A_g[:, :, c], A_o[:, :, c]) < 1e-10
+    for c in range(3):
+        assert rel(S_g[:, :, c][..., ~cross], S_o[:, :, c][..., ~cross]) < 1e-10
+        scale = np.abs(S_o[:, :, c]).max()
+        assert np.abs(S_g[:, :, c][..., cross] - S_o[:, :, c][..., cross]).max() < 0.05 * scale
+
+
+def test_c2_spectrum_and_apply_match_oracle(c2, orc):
+    import torch
+    m, sig, op, S_g, A_g = c2
+    sh_g, ah_g = op.get_ie_kernel_spectral()
+    sh_o, ah_o = orc.tensor_spectrum(m.Nx, m.Ny, m.Nz, S_g, A_g)
+    assert rel(sh_g, sh_o) < 1e-12 and rel(ah_g, ah_o) < 1e-12
+    csiga = csiga_from_sigma(sig, m.freq)
+    csigb, sqsigb = orc.background_cells(m)
+    v = random_vec(m, 21)
+    ref = orc.apply(m.Nx, m.Ny, m.Nz, sh_o, ah_o, csiga, csigb, sqsigb, m.dz, v)
+    assert rel(op.apply_precond(v), ref) < 1e-12
+    x = torch.from_numpy(v.ravel()).to("cuda", torch.complex64)
+    y = torch.empty_like(x)
+    op.apply_device(x.data_ptr(), y.data_ptr(), 1)
+    op.check_device_error()
+    assert rel(y.cpu().numpy().astype(np.complex128).reshape(ref.shape), ref) < 2e-5
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-8), (1, 1e-6)])
+def test_c2_solution_satisfies_the_system(c2, orc, precision, tol):
+    """SolveEquation: E = a chi with A chi = sqrt(Re sigma_b) E0; the residual is recomputed in FP64 on the
+    CPU from the GPU's solution."""
+    m, sig, op, S_g, A_g = c2
+    sh, ah = op.get_ie_kernel_spectral()
+    csiga = csiga_from_sigma(sig, m.freq)
+    csigb, sqsigb = orc.background_cells(m)
+    for pol in (1, 0):
+        E0 = plane_wave_integral(m, pol)
+        E, info = op.solve_equation(E0, tol=tol, precision=precision)
+        assert info.stat == 1 and info.be < tol
+        a = 2.0 * sqsigb[:, None, None] / (csiga + np.conj(csigb)[:, None, None])
+        chi = E / a[None]
+        rhs = sqsigb[None, :, None, None] * E0
+        r = orc.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, chi) - rhs
+        assert np.linalg.norm(r) / np.linalg.norm(rhs) < 1.5 * tol
