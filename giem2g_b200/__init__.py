@@ -82,6 +82,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_rc_get_kernel", "giem2g_rc_set_anomaly_conductivity", "giem2g_rc_recalculate",
     "giem2g_rc_recalculate_device", "giem2g_rc_get_stream", "giem2g_rc_delete", "giem2g_set_precision",
     "giem2g_set_preconditioner", "giem2g_preconditioner_calls", "giem2g_apply_preconditioner",
+    "giem2g_selftest_bounded_wait",
 ]
 
 
@@ -153,6 +154,7 @@ def lib():
     L.giem2g_preconditioner_calls.argtypes = [vp]
     L.giem2g_preconditioner_calls.restype = ctypes.c_longlong
     L.giem2g_apply_preconditioner.argtypes = [vp, vp, vp]
+    L.giem2g_selftest_bounded_wait.argtypes = [ip]
     L.giem2g_set_kernel_timing.argtypes = [vp, ip]
     L.giem2g_last_contract_ms.argtypes = [vp]
     L.giem2g_last_contract_ms.restype = dp

@@ -257,6 +257,11 @@ int giem2g_rc_recalculate_device(void *rc, const void *d_E, void *d_Ea, void *d_
 void *giem2g_rc_get_stream(void *rc);
 void giem2g_rc_delete(void *rc);
 
+/* Failure-detection self-test (no counterpart in the reference): runs the library's bounded wait on an
+ * mbarrier that nothing completes, with a limit of limit_ms (1..2000); returns the device error code the
+ * wait recorded (77) after about limit_ms, or a negative status.  The context stays usable. */
+int giem2g_selftest_bounded_wait(int limit_ms);
+
 #ifdef __cplusplus
 }
 #endif
