@@ -48,8 +48,11 @@ def test_nan_right_hand_side_reports_numeric_status(g2lib, precision):
 
 
 def test_corrupt_tensor_reports_numeric_status(g2lib):
-    m, op = _op(g2lib)
-    S, A = op.get_ie_kernel_spatial()
+    m, sig = config_small_block()
+    op = g2lib.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    S, A = op.get_ie_kernel_spatial()  # the spectral transform works in place: take the spatial tensor first
+    op.set_anomaly_sigma(sig, m.freq)
     Sb = S.copy()
     Sb[1, 2, 0, 3] = np.inf
     op.set_ie_kernel_spatial(Sb, A)
