@@ -551,14 +551,16 @@ class Batch:
         return [self._info(i, res[i]) for i in range(self.n)]
 
     def solve(self, E_bkg, E0=None, tol=1e-6):
-        """Host arrays (complex128, (3,Nz,Ny,Nx) each); returns (list of solutions, list of SolveInfo)."""
+        """Host arrays (complex128, (3,Nz,Ny,Nx) each); E0 is None or a list whose entries may be None (no
+        guess for that instance).  Returns (list of solutions, list of SolveInfo)."""
         ins = [_c128(e) for e in E_bkg]
         outs = [np.empty_like(e) for e in ins]
-        e0 = [_c128(e) for e in E0] if E0 is not None else None
+        e0 = [_c128(e) if e is not None else None for e in E0] if E0 is not None else None
         res = (ResultT * self.n)()
         rc = lib().giem2g_solve_batched(self.handle, _ptrs([a.ctypes.data for a in ins]),
                                         _ptrs([a.ctypes.data for a in outs]),
-                                        _ptrs([a.ctypes.data for a in e0]) if e0 is not None else None,
+                                        _ptrs([a.ctypes.data if a is not None else None for a in e0])
+                                        if e0 is not None else None,
                                         self._ctl(tol), res)
         _check(rc, "giem2g_solve_batched")
         return outs, [self._info(i, res[i]) for i in range(self.n)]

@@ -5,7 +5,8 @@
 Restates the solve part of the reference's main program (giem2g.F90:336-373, 430-470): read the JSON
 input (background, anomaly grid and conductivity file, frequencies, FGMRES settings), then for every
 frequency in order build the Green's tensor on the GPU, transform it, set the anomaly conductivity and
-solve the plane-wave problem for EY, then EX.  The initial guess of each solve follows the reference:
+solve the plane-wave problem for EY and EX (as one lockstep batch of the two polarisations by default, or
+one after the other with --sequential, as the reference does).  The initial guess of each solve follows the reference:
 a solution file of the same frequency and polarisation if one exists in the output directory, else
 nothing for the first frequency, else the previous frequency's solution of that polarisation.  With
 "Save Solution" true every solution is written as SOL_P{Y,X}_F<freq>.bin.  With "Recalculate Fields"
@@ -48,8 +49,11 @@ def model_from_input(inp: dict, base_dir: str):
     return m, sig, freqs, ctl
 
 
-def run(input_path: str, precision: int = 0, outdir: str | None = None, log=print, warm_start: bool = True) -> dict:
-    from . import IEOperator, RCOperator
+def run(input_path: str, precision: int = 0, outdir: str | None = None, log=print, warm_start: bool = True,
+        batched: bool = True) -> dict:
+    """batched: solve the two polarisations of each frequency as one lockstep batch (the same iterates as
+    two single solves; in mixed precision their complex64 applies share every tensor read)."""
+    from . import Batch, IEOperator, RCOperator
     from .sources import plane_wave_integral, plane_wave_points
     inp = load_input(input_path)
     base = os.path.dirname(os.path.abspath(input_path))
@@ -71,6 +75,7 @@ def run(input_path: str, precision: int = 0, outdir: str | None = None, log=prin
         out["receivers"] = {"depth": zr_used.tolist(), "xshift": xs, "yshift": ys}
     op = IEOperator.from_model(m0) if solve else None
     prev = {EY: None, EX: None}
+    pols = (EY, EX)
     try:
         for i, f in enumerate(freqs):
             m = m0.with_freq(f)
@@ -84,46 +89,67 @@ def run(input_path: str, precision: int = 0, outdir: str | None = None, log=prin
                 rc.calc_fft_of_rc_kernel()
                 rc.set_anomaly_sigma(sig, f)
             t_setup = time.perf_counter() - t0
-            for pol in (EY, EX):
-                name = os.path.join(outdir, solution_name(pol, f))
-                guess = load_solution(name, m.Nx, m.Ny, m.Nz)
-                row = {"freq": f, "pol": "EY" if pol == EY else "EX", "setup_s": t_setup}
-                if solve:
-                    source = "file" if guess is not None else ("previous frequency" if i > 0 else "none")
-                    if guess is None and i > 0 and warm_start:
-                        guess = prev[pol]
-                    elif guess is None:
-                        source = "none"
-                    E_bkg = plane_wave_integral(m, pol)
-                    E, info = op.solve_equation(E_bkg, E0=guess, tol=ctl["tol"], max_restart=ctl["max_restart"],
-                                                outer_buf=ctl["outer_buf"], inner_buf=ctl["inner_buf"],
-                                                precision=precision)
-                    prev[pol] = E
-                    if save:
-                        save_solution(name, E)
-                    row.update({"guess": source, "iterations": info.iterations, "stat": info.stat,
-                                "true_rel_residual": info.be, "device_ms": info.device_ms})
+            names = {pol: os.path.join(outdir, solution_name(pol, f)) for pol in pols}
+            rows = {pol: {"freq": f, "pol": "EY" if pol == EY else "EX", "setup_s": t_setup} for pol in pols}
+            fields = {}
+            if solve:
+                # initial guesses (giem2g.F90:356-373): the file of this frequency, else the previous frequency
+                guesses, sources = {}, {}
+                for pol in pols:
+                    g = load_solution(names[pol], m.Nx, m.Ny, m.Nz)
+                    src = "file" if g is not None else ("previous frequency" if i > 0 and warm_start else "none")
+                    if g is None and i > 0 and warm_start:
+                        g = prev[pol]
+                    guesses[pol], sources[pol] = g, src
+                E_bkg = {pol: plane_wave_integral(m, pol) for pol in pols}
+                if batched:
+                    b = Batch([op, op], outer_buf=ctl["outer_buf"], inner_buf=ctl["inner_buf"], precision=precision,
+                              max_restart=ctl["max_restart"])
+                    try:
+                        sols, infos = b.solve([E_bkg[p] for p in pols], E0=[guesses[p] for p in pols], tol=ctl["tol"])
+                    finally:
+                        b.delete()
+                    results = dict(zip(pols, zip(sols, infos)))
                 else:
-                    if guess is None:  # giem2g.F90:398-412: "Solution not found", next frequency
-                        row["solution"] = "not found"
-                        out["solves"].append(row)
-                        if log:
-                            log(json.dumps(row))
+                    results = {pol: op.solve_equation(E_bkg[pol], E0=guesses[pol], tol=ctl["tol"],
+                                                      max_restart=ctl["max_restart"], outer_buf=ctl["outer_buf"],
+                                                      inner_buf=ctl["inner_buf"], precision=precision)
+                               for pol in pols}
+                for pol in pols:
+                    E, info = results[pol]
+                    prev[pol] = fields[pol] = E
+                    if save:
+                        save_solution(names[pol], E)
+                    rows[pol].update({"guess": sources[pol], "iterations": info.iterations, "stat": info.stat,
+                                      "true_rel_residual": info.be, "device_ms": info.device_ms,
+                                      "batched": bool(batched)})
+            else:
+                for pol in pols:
+                    g = load_solution(names[pol], m.Nx, m.Ny, m.Nz)
+                    if g is None:  # giem2g.F90:398-412: "Solution not found", next frequency
+                        rows[pol]["solution"] = "not found"
                         break
-                    E = guess
-                    row["solution"] = "file"
+                    fields[pol] = g
+                    rows[pol]["solution"] = "file"
+            for pol in pols:
+                if pol not in fields:
+                    if "solution" in rows[pol]:
+                        out["solves"].append(rows[pol])
+                        if log:
+                            log(json.dumps(rows[pol]))
+                    break
                 if rc is not None:
                     t1 = time.perf_counter()
-                    Ea, Ha = rc.recalculate(E)
+                    Ea, Ha = rc.recalculate(fields[pol])
                     F = plane_wave_points(m, pol, zr_used)  # [Nr, 6]: Ex Ey Ez Hx Hy Hz
                     Et = Ea + F[:, :3].T[None, None]
                     Ht = Ha + F[:, 3:].T[None, None]
                     save_receiver_fields(os.path.join(outdir, receiver_output_name(pol, f)), m.dx, m.dy, zr_used, xs,
                                          ys, f, Ea, Ha, Et, Ht)
-                    row["recalc_s"] = time.perf_counter() - t1
-                out["solves"].append(row)
+                    rows[pol]["recalc_s"] = time.perf_counter() - t1
+                out["solves"].append(rows[pol])
                 if log:
-                    log(json.dumps(row))
+                    log(json.dumps(rows[pol]))
     finally:
         if op is not None:
             op.delete()
@@ -138,8 +164,9 @@ def main(argv=None):
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1], help="0: FP64, 1: mixed")
     ap.add_argument("--outdir", default=None, help="directory of the SOL_*.bin files (default: cwd)")
     ap.add_argument("--cold", action="store_true", help="no previous-frequency guess (for comparison)")
+    ap.add_argument("--sequential", action="store_true", help="solve EY then EX one at a time, as the reference does")
     args = ap.parse_args(argv)
-    res = run(args.input, args.precision, args.outdir, warm_start=not args.cold)
+    res = run(args.input, args.precision, args.outdir, warm_start=not args.cold, batched=not args.sequential)
     print(json.dumps(res))
 
 

@@ -53,6 +53,16 @@ def test_driver_frequency_loop_files_and_warm_start(g2lib, tmp_path):
     op.delete()
     E_file = load_solution(str(tmp_path / solution_name(EX, 3.0)), 16, 16, 8)
     assert np.linalg.norm(E_file - E_cold) / np.linalg.norm(E_cold) < 1e-6
+    # the reference's order (EY, then EX, one at a time) gives the same solutions as the batched default
+    seq_dir = tmp_path / "sequential"
+    seq_dir.mkdir()
+    seq = run(path, precision=0, outdir=str(seq_dir), log=None, batched=False)
+    assert [r["iterations"] for r in seq["solves"]] == [r["iterations"] for r in rows]
+    for f in freqs:
+        for pol in (EY, EX):
+            a = load_solution(str(seq_dir / solution_name(pol, f)), 16, 16, 8)
+            b = load_solution(str(tmp_path / solution_name(pol, f)), 16, 16, 8)
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-10
     # a second run starts every solve from its own solution file: nothing left to iterate
     again = run(path, precision=0, outdir=str(tmp_path), log=None)
     assert all(r["guess"] == "file" and r["stat"] == 1 and r["iterations"] <= 1 for r in again["solves"])
