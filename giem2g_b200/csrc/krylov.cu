@@ -25,6 +25,7 @@
 namespace {
 
 constexpr int kVT = 256;   // threads of the vector kernels
+constexpr int kILP = 4;    // elements per thread and iteration of the element-wise vector kernels
 constexpr int KMAX = 32;   // largest basis handled in one sweep
 constexpr double ZERO_THRESHOLD = 1e-14;  // gmres.F90:21
 constexpr int N_IGS = 3;                  // gmres.F90:22
@@ -306,7 +307,17 @@ __global__ void __launch_bounds__(kVT) k_scale_finish(C *v, const C *w, size_t N
 {
     if (gate && *gate == 0) return;
     const double inv = 1.0 / L.scal[S_DNORMW];
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+    // kILP independent elements per thread and iteration, loads first: more bytes in flight per SM
+    const size_t S = (size_t)gridDim.x * kVT;
+    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
+    for (; i + (kILP - 1) * S < N; i += kILP * S) {
+        double2 x[kILP];
+#pragma unroll
+        for (int u = 0; u < kILP; u++) x[u] = ld2(w, i + u * S);
+#pragma unroll
+        for (int u = 0; u < kILP; u++) st2(v, i + u * S, make_double2(x[u].x * inv, x[u].y * inv));
+    }
+    for (; i < N; i += S) {
         const double2 x = ld2(w, i);
         st2(v, i, make_double2(x.x * inv, x.y * inv));
     }
@@ -388,16 +399,29 @@ __global__ void __launch_bounds__(kVT) k_axpby(CO *out, double a, const CX *x, d
                                                const int *gate)
 {
     if (gate && *gate == 0) return;
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
-        const double2 xv = ld2(x, i);
+    auto elem = [&](double2 xv, double2 yv) {
         double2 r = make_double2(a * xv.x, a * xv.y);
         if (y) {
-            const double2 yv = ld2(y, i);
             r.x += b * yv.x;
             r.y += b * yv.y;
         }
-        st2(out, i, r);
+        return r;
+    };
+    // kILP independent elements per thread and iteration, loads first (out may alias x or y: every
+    // element is still read before it is written, by the same thread)
+    const size_t S = (size_t)gridDim.x * kVT;
+    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
+    for (; i + (kILP - 1) * S < N; i += kILP * S) {
+        double2 xv[kILP], yv[kILP];
+#pragma unroll
+        for (int u = 0; u < kILP; u++) {
+            xv[u] = ld2(x, i + u * S);
+            yv[u] = y ? ld2(y, i + u * S) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kILP; u++) st2(out, i + u * S, elem(xv[u], yv[u]));
     }
+    for (; i < N; i += S) st2(out, i, elem(ld2(x, i), y ? ld2(y, i) : make_double2(0.0, 0.0)));
 }
 // x = v, or x = 0 when ||v|| < ZERO_THRESHOLD (gmres.F90:139-145)
 template <typename C>
