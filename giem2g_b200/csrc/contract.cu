@@ -267,6 +267,241 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
 }
 
 // ------------------------------------------------------------------------------------------------
+// Barrier-free form: the j-slices of a row sit in one warp and are reduced with shuffles.
+//
+// Threads (g, w, lane): warp group g takes the CTA's units (tickets) it = g, g + NG, ...; warp w of the
+// group owns rows z = w*ZW + zl, and lane = zl + ZW*s sums j = s, s + SL, s + 2 SL, ... (interleaved
+// slices: the SL lanes of one zl read SL consecutive spectrum entries, one wavefront).  Ticket it uses
+// stage it % NSTAGE in round it / NSTAGE.  A parity wait cannot tell round r from round r-2, and with
+// several groups on one ring a group could reach round r of a stage while round r-1 (another group's
+// ticket) is still in flight.  So tickets are passed in order: a warp starts waiting for ticket it only
+// once ticket it-1 has been passed (a shared counter raised with atomicMax), which by induction means
+// round r-1 of its stage has landed and the parity wait is exact.  After its last shared-memory read
+// every lane arrives on the stage's empty barrier (it counts the group's threads), so the producer
+// refills the stage while the warp reduces.  The reduction is a recursive halving over the lane bits of
+// s: each step sends half of the outputs a lane still holds to its partner and adds the half it
+// receives, so every lane ends with NR/SL of the NR = 2*3*PTS reals and stores them.  No CTA-wide
+// barrier is left in the consumer loop: one warp's reduction and stores overlap another's FMAs.
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB>
+struct CfgL {
+    static constexpr int P = NZ * (NZ + 1) / 2;
+    static constexpr int T = 4 * P + 2 * NZ * NZ;
+    static constexpr int Z3 = 3 * NZ;
+    static constexpr int PTS = 4 * NP;
+    static constexpr int ZW = 32 / SL;   // rows per warp
+    static constexpr int W = NZ / ZW;    // warps per group
+    static constexpr int NC = NG * W * 32;
+    static constexpr int NTHREADS = NC + 32;
+    static constexpr int JS = NZ / SL;
+    static constexpr int ES = 2 * sizeof(R);
+    static constexpr int TBYTES = T * ES;
+    static constexpr int UBYTES = PTS * Z3 * ES;
+    static constexpr int STAGE_BYTES = TBYTES + UBYTES;
+    static constexpr int NR = 2 * 3 * PTS;  // reals per lane before the reduction
+    static constexpr int HR = NR / SL;      // reals per lane after it
+    static constexpr int SMEM = NSTAGE * STAGE_BYTES + 2 * NSTAGE * 8 + 16;  // + ticket counter
+    static_assert(32 % SL == 0 && NZ % ZW == 0, "slices must tile a warp and warps the rows");
+    static_assert(NR % SL == 0 && HR % 2 == 0, "every lane must end with whole complex outputs");
+    static_assert(STAGE_BYTES % 16 == 0 && TBYTES % 16 == 0, "bulk copies need 16-byte multiples");
+    static_assert(SMEM <= 232448, "exceeds the 227 KB dynamic shared memory of one CTA");
+    static_assert(MINB * (SMEM + 1024) <= 233472, "MINB CTAs do not fit the SM's shared memory");
+};
+
+// one halving step over lane bit B of the slice index, then the next; v[0, LEN) is still held
+template <int B, int LEN, int ZW, int SL, int NR, typename R>
+G2_D void halve_slices(R (&v)[NR], int s, int &f0)
+{
+    if constexpr ((1 << B) < SL) {
+        constexpr int HALF = LEN / 2;
+        const bool up = (s >> B) & 1;
+#pragma unroll
+        for (int i = 0; i < HALF; i++) {
+            const R send = up ? v[i] : v[HALF + i];
+            const R keep = up ? v[HALF + i] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, ZW << B);
+        }
+        if (up) f0 += HALF;
+        halve_slices<B + 1, HALF, ZW, SL, NR>(v, s, f0);
+    }
+}
+
+// Spin (bounded, 2 s) until ticket it-1 has been passed.
+G2_D bool wait_ticket(const int *passed, int it, int *err)
+{
+    const volatile int *p = passed;
+    if (*p >= it) return true;
+    const uint64_t t0 = globaltimer_ns();
+    while (*p < it) {
+        if (globaltimer_ns() - t0 > 2000000000ull) {
+            atomicCAS(err, 0, 17);
+            return false;
+        }
+    }
+    return true;
+}
+
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4>
+__global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREADS, MINB)
+    k_contract_wl(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
+                  long long nunits, int *err, const int *gate)
+{
+    if (gate && *gate == 0) return;  // uniform across the CTA: nothing has been issued yet
+    using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>;
+    constexpr int PTS = Cfg::PTS, ZW = Cfg::ZW, W = Cfg::W, P = Cfg::P;
+    using C2 = typename V2<R>::T;
+    constexpr int AW = sizeof(R) == 8 ? asw_width64(NZ) : asw_width32(NZ);
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *stages = smem;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * Cfg::STAGE_BYTES);
+    uint64_t *empty = full + NSTAGE;
+    int *passed = reinterpret_cast<int *>(empty + NSTAGE);  // tickets [0, *passed) have been passed
+
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < NSTAGE; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], W * 32);
+        }
+        *passed = 0;
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const long long first = blockIdx.x, stride = gridDim.x;
+    const long long my_n = first < nunits ? (nunits - 1 - first) / stride + 1 : 0;
+
+    if (tid >= Cfg::NC) {
+        // producer warp: one lane streams units (tensor + 4-point spectra) into the stage ring in order
+        if (tid == Cfg::NC) {
+            const uint64_t pol_t = l2_policy_evict_first();
+            const uint64_t pol_u = l2_policy_evict_last();
+            long long issued = 0;
+            bool ok = true;
+            for (long long it = 0; it < my_n; it++) {
+                const int slot = (int)(it % NSTAGE);
+                const uint32_t round = (uint32_t)(it / NSTAGE);
+                if (round > 0) {
+                    if (!mbar_wait_bounded(&empty[slot], (round - 1) & 1, err, 14)) { ok = false; break; }
+                }
+                const long long unit = first + it * stride;
+                unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
+                mbar_arrive_expect_tx(&full[slot], Cfg::STAGE_BYTES);
+                bulk_g2s(st, G + unit * (long long)Cfg::T, Cfg::TBYTES, &full[slot], pol_t);
+                bulk_g2s(st + Cfg::TBYTES, Uhat + unit * (long long)PTS * Cfg::Z3, Cfg::UBYTES, &full[slot], pol_u);
+                issued++;
+            }
+            if (!ok) {
+                for (long long it = (issued > NSTAGE ? issued - NSTAGE : 0); it < issued; it++)
+                    mbar_wait_bounded(&full[it % NSTAGE], (uint32_t)(it / NSTAGE) & 1, err, 16);
+            }
+        }
+        return;
+    }
+
+    const int warp = tid >> 5, lane = tid & 31;
+    const int g = warp / W, z = (warp % W) * ZW + lane % ZW, s = lane / ZW;
+    for (long long it = g; it < my_n; it += NG) {
+        const int slot = (int)(it % NSTAGE);
+        const uint32_t round = (uint32_t)(it / NSTAGE);
+        // the warp leaves together (its lanes shuffle with one another below)
+        if (!__all_sync(0xffffffffu, wait_ticket(passed, (int)it, err))) return;
+        __threadfence_block();
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[slot], round & 1, err, 15))) return;
+        __threadfence_block();
+        if (lane == 0) atomicMax(passed, (int)it + 1);
+        const unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
+        const C2 *gb = reinterpret_cast<const C2 *>(st);
+        const C2 *ub = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);  // [pt][c][j]
+        constexpr int NA = M4 ? 2 : 3;
+        R acc[3][PTS][NA];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int p = 0; p < PTS; p++)
+#pragma unroll
+                for (int k = 0; k < NA; k++) acc[c][p][k] = R(0);
+        const C2 *gxx = gb, *gxy = gb + P, *gyy = gb + 2 * P, *gzz = gb + 3 * P;
+        const C2 *gxz = gb + 4 * P, *gyz = gb + 4 * P + NZ * NZ;
+#pragma unroll 2
+        for (int jj = 0; jj < Cfg::JS; jj++) {
+            const int j = jj * SL + s;
+            const int si = sym_idx<NZ>(z, j);
+            const int a_zj = asw(z, j, NZ, AW), a_jz = asw(j, z, NZ, AW);
+            const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[a_zj], gyz[a_zj], gxz[a_jz], gyz[a_jz]};
+            C2 u[PTS][3];
+            R ue[PTS][3];
+#pragma unroll
+            for (int p = 0; p < PTS; p++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    u[p][c] = ub[(p * 3 + c) * NZ + j];
+                    ue[p][c] = u[p][c].x + u[p][c].y;
+                }
+            // sign table as in k_contract_tma; point p = slot * NP + vector, slot bits (sx, m)
+#define G2_TERM_L(C, K, IN, SGN)                                                 \
+    {                                                                            \
+        const R es_ = e[K].x + e[K].y;                                           \
+        _Pragma("unroll") for (int p = 0; p < PTS; p++)                          \
+        {                                                                        \
+            const int sl_ = p / NP;                                              \
+            const R sx = (sl_ & 2) ? R(-1) : R(1);                               \
+            const R m = (sl_ & 1) ? R(-1) : R(1);                                \
+            const R sg = (SGN);                                                  \
+            if constexpr (M4) {                                                  \
+                acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);       \
+                acc[C][p][0] = fma(-sg * e[K].y, u[p][IN].y, acc[C][p][0]);      \
+                acc[C][p][1] = fma(sg * e[K].x, u[p][IN].y, acc[C][p][1]);       \
+                acc[C][p][1] = fma(sg * e[K].y, u[p][IN].x, acc[C][p][1]);       \
+            } else {                                                             \
+                acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);       \
+                acc[C][p][1] = fma(sg * e[K].y, u[p][IN].y, acc[C][p][1]);       \
+                acc[C][p][NA - 1] = fma(sg * es_, ue[p][IN], acc[C][p][NA - 1]); \
+            }                                                                    \
+        }                                                                        \
+    }
+            G2_TERM_L(0, 0, 0, R(1))
+            G2_TERM_L(1, 1, 0, sx * m)
+            G2_TERM_L(2, 6, 0, -sx)
+            G2_TERM_L(0, 1, 1, sx * m)
+            G2_TERM_L(1, 2, 1, R(1))
+            G2_TERM_L(2, 7, 1, -m)
+            G2_TERM_L(0, 4, 2, sx)
+            G2_TERM_L(1, 5, 2, m)
+            G2_TERM_L(2, 3, 2, R(1))
+#undef G2_TERM_L
+        }
+        mbar_arrive(&empty[slot]);  // this lane's reads of the stage are done
+
+        R v[Cfg::NR];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int p = 0; p < PTS; p++) {
+                if constexpr (M4) {
+                    v[2 * (c * PTS + p)] = acc[c][p][0];
+                    v[2 * (c * PTS + p) + 1] = acc[c][p][1];
+                } else {
+                    const R t1 = acc[c][p][0], t2 = acc[c][p][1], t3 = acc[c][p][NA - 1];
+                    v[2 * (c * PTS + p)] = t1 - t2;
+                    v[2 * (c * PTS + p) + 1] = t3 - t1 - t2;
+                }
+            }
+        int f0 = 0;  // first flat output index this lane keeps
+        halve_slices<0, Cfg::NR, ZW, SL, Cfg::NR>(v, s, f0);
+        const long long unit = first + it * stride;
+        const int q = (int)(unit / Ny), r = (int)(unit - (long long)q * Ny);
+        C2 *dst = Uhat + unit * PTS * Cfg::Z3 + z;
+#pragma unroll
+        for (int i = 0; i < Cfg::HR; i += 2) {
+            const int k = (f0 + i) >> 1, c = k / PTS, p = k - c * PTS, sl = p / NP;
+            C2 o{v[i], v[i + 1]};
+            if ((q == 0 && (sl & 2)) || (r == 0 && (sl & 1))) o = C2{R(0), R(0)};
+            dst[(p * 3 + c) * NZ] = o;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // complex64 contraction in the Walsh basis of the four points, with packed FP32 pair arithmetic.
 //
 // The four points of a unit, p = (sx bit, m bit), form the group Z2 x Z2 and every term of the sign table
@@ -539,6 +774,25 @@ int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cud
     return G2_OK;
 }
 
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP = 1, int MINB = 1, bool M4 = false>
+int launch_wl(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
+{
+    using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>;
+    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4>;
+    nsm *= MINB;
+    static bool attr = false;
+    if (!attr) {
+        G2_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+        attr = true;
+    }
+    const long long units = (long long)Nx * Ny;
+    const int grid = (int)(units < nsm ? units : nsm);
+    kern<<<grid, Cfg::NTHREADS, Cfg::SMEM, st>>>(reinterpret_cast<const typename V2<R>::T *>(G),
+                                                 reinterpret_cast<typename V2<R>::T *>(Uhat), Ny, units, err, gate);
+    G2_CUDA_CHECK(cudaGetLastError());
+    return G2_OK;
+}
+
 int sm_count()
 {
     static int n = 0;
@@ -556,8 +810,8 @@ int sm_count()
 // on the operator's own buffers and stores its pick in the operator.
 int ie_contract_variants(int precision, int Nz)
 {
-    if (precision == 0) return Nz == 32 ? 5 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
-    return Nz == 32 ? 14 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    if (precision == 0) return Nz == 32 ? 11 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
+    return Nz == 32 ? 21 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
@@ -574,6 +828,12 @@ int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, 
         if (v == 2) return launch_cfg<double, 32, 4, 1, 1, 1, false, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 3) return launch_cfg<double, 32, 2, 1, 1, 1, false, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 4) return launch_cfg<double, 32, 4, 1, 1, 1, false, 3, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 5) return launch_wl<double, 32, 4, 2, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 6) return launch_wl<double, 32, 4, 3, 3, 1, 1, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 7) return launch_wl<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 8) return launch_wl<double, 32, 2, 3, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 9) return launch_wl<double, 32, 2, 4, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 10) return launch_wl<double, 32, 4, 2, 3, 1, 1, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<double, 32, 8, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
     }
@@ -605,6 +865,13 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         case 11: return launch_w32<32, 4, 1, 2, 1, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 12: return launch_cfg<float, 32, 4, 1, 2, 1, false, 3, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 13: return launch_cfg<float, 32, 4, 1, 3, 1, false, 2, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 14: return launch_wl<float, 32, 4, 3, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 15: return launch_wl<float, 32, 4, 2, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 16: return launch_wl<float, 32, 2, 4, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 17: return launch_wl<float, 32, 4, 4, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 18: return launch_wl<float, 32, 2, 6, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 19: return launch_wl<float, 32, 2, 5, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 20: return launch_wl<float, 32, 1, 8, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
         default: return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
         }
     case 48:
@@ -618,7 +885,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 9 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 14 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -641,6 +908,11 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         if (v == 6) return launch_cfg<float, 32, 2, 1, 1, 2, true, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 7) return launch_w32<32, 4, 1, 2, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 8) return launch_cfg<float, 32, 4, 1, 2, 2, false, 2, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 9) return launch_wl<float, 32, 4, 2, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 10) return launch_wl<float, 32, 8, 1, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 11) return launch_wl<float, 32, 2, 4, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 12) return launch_wl<float, 32, 2, 5, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 13) return launch_wl<float, 32, 2, 3, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 32, 4, 2, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);

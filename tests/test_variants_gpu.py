@@ -1,7 +1,9 @@
 """Every contraction tile variant (FP64, complex64, paired complex64) against the oracle apply.
 
 The autotuner may pick any variant, so each one must meet the apply tolerances: 1e-12 (complex128) and
-2e-5 (complex64) relative to the oracle.
+2e-5 (complex64) relative to the oracle.  The small grids give each persistent CTA at most one unit; the
+larger ones (thousands of units over the SMs) run every stage ring through many rounds, the steady state
+of the benchmark grid.
 """
 import numpy as np
 import pytest
@@ -12,7 +14,8 @@ from tests.helpers import random_sigma, random_spatial_tensor, random_vec, rel, 
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("shape", [(8, 8, 8), (4, 8, 16), (4, 4, 32), (2, 4, 48)])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (4, 8, 16), (4, 4, 32), (2, 4, 48),
+                                   (128, 64, 8), (64, 64, 16), (64, 32, 32), (32, 32, 48)])
 def test_all_contraction_variants(g2lib, orc, shape):
     import torch
     m = tiny_model(*shape)
