@@ -238,8 +238,8 @@ def run_b200(args, rank, world, local_rank):
     d_sol_x = torch.empty_like(d_ex)
 
     # contraction tile shape: time the variants once (autotuner) and keep the fastest
-    from giem2g_b200.autotune import autotune_contraction
-    tuned = autotune_contraction(op)
+    from giem2g_b200.autotune import autotune_contraction, pin_contraction
+    tuned = pin_contraction(op, args.variants) if args.variants else autotune_contraction(op)
 
     def solve_pair(prec, tol=TOL):
         iy = op.solve_device(d_ey.data_ptr(), d_sol_y.data_ptr(), None, tol=tol, max_restart=MAXRESTART,
@@ -512,6 +512,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variants", default=None,
+                    help="pin the tile shapes instead of autotuning: v64,v32,vpair[,fft_lines] (for profilers)")
     args = ap.parse_args()
     rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":

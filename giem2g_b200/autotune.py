@@ -93,3 +93,23 @@ def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> di
         except Exception:
             pass
     return {str(k): v for k, v in picks.items()}
+
+
+def pin_contraction(op, spec: str) -> dict:
+    """Set the tile shapes by hand instead of timing them: spec = "v64,v32,vpair[,fft_lines]" (the
+    variant numbers the tuner reports).  Profilers need it, because timings taken under a profiler pick
+    other shapes than the plain run does."""
+    parts = [int(t) for t in spec.split(",")]
+    if len(parts) not in (3, 4):
+        raise ValueError("expected v64,v32,vpair[,fft_lines]")
+    picks = {}
+    for prec, v in enumerate(parts[:3]):
+        if op.contract_variants(prec) > 1:
+            if not 0 <= v < op.contract_variants(prec):
+                raise ValueError(f"variant {v} out of range for precision {prec}")
+            op.set_contract_variant(prec, v)
+        picks[str(prec)] = {"variant": v, "ms": None, "pinned": True}
+    if len(parts) == 4:
+        op.set_fft_lines(parts[3])
+        picks["fft_lines"] = {"lines": parts[3], "ms": None, "pinned": True}
+    return picks

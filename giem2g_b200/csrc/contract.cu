@@ -340,7 +340,8 @@ G2_D bool wait_ticket(const int *passed, int it, int *err)
     return true;
 }
 
-template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4>
+// PK (complex64): the packed 3-multiply form of k_contract_tma, two instructions per complex multiply-add.
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4, bool PK>
 __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREADS, MINB)
     k_contract_wl(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
                   long long nunits, int *err, const int *gate)
@@ -412,14 +413,18 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
         const unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
         const C2 *gb = reinterpret_cast<const C2 *>(st);
         const C2 *ub = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);  // [pt][c][j]
+        static_assert(!PK || (sizeof(R) == 4 && !M4), "packed pairs are a complex64 3-multiply form");
         constexpr int NA = M4 ? 2 : 3;
         R acc[3][PTS][NA];
+        C2 accp[3][PTS];  // PK: (t1, t2) of the 3-multiply form
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
-            for (int p = 0; p < PTS; p++)
+            for (int p = 0; p < PTS; p++) {
+                accp[c][p] = C2{R(0), R(0)};
 #pragma unroll
                 for (int k = 0; k < NA; k++) acc[c][p][k] = R(0);
+            }
         const C2 *gxx = gb, *gxy = gb + P, *gyy = gb + 2 * P, *gzz = gb + 3 * P;
         const C2 *gxz = gb + 4 * P, *gyz = gb + 4 * P + NZ * NZ;
 #pragma unroll 2
@@ -428,6 +433,9 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
             const int si = sym_idx<NZ>(z, j);
             const int a_zj = asw(z, j, NZ, AW), a_jz = asw(j, z, NZ, AW);
             const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[a_zj], gyz[a_zj], gxz[a_jz], gyz[a_jz]};
+            C2 en[8];  // PK: negated copies (only the ones a negative sign uses survive compilation)
+#pragma unroll
+            for (int k = 0; k < 8; k++) en[k] = C2{-e[k].x, -e[k].y};
             C2 u[PTS][3];
             R ue[PTS][3];
 #pragma unroll
@@ -447,7 +455,10 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
             const R sx = (sl_ & 2) ? R(-1) : R(1);                               \
             const R m = (sl_ & 1) ? R(-1) : R(1);                                \
             const R sg = (SGN);                                                  \
-            if constexpr (M4) {                                                  \
+            if constexpr (PK) {                                                  \
+                accp[C][p] = ffma2(sg < R(0) ? en[K] : e[K], u[p][IN], accp[C][p]); \
+                acc[C][p][NA - 1] = fma(sg * es_, ue[p][IN], acc[C][p][NA - 1]); \
+            } else if constexpr (M4) {                                           \
                 acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);       \
                 acc[C][p][0] = fma(-sg * e[K].y, u[p][IN].y, acc[C][p][0]);      \
                 acc[C][p][1] = fma(sg * e[K].x, u[p][IN].y, acc[C][p][1]);       \
@@ -477,7 +488,11 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
         for (int c = 0; c < 3; c++)
 #pragma unroll
             for (int p = 0; p < PTS; p++) {
-                if constexpr (M4) {
+                if constexpr (PK) {
+                    const R t1 = accp[c][p].x, t2 = accp[c][p].y, t3 = acc[c][p][NA - 1];
+                    v[2 * (c * PTS + p)] = t1 - t2;
+                    v[2 * (c * PTS + p) + 1] = t3 - t1 - t2;
+                } else if constexpr (M4) {
                     v[2 * (c * PTS + p)] = acc[c][p][0];
                     v[2 * (c * PTS + p) + 1] = acc[c][p][1];
                 } else {
@@ -774,11 +789,11 @@ int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cud
     return G2_OK;
 }
 
-template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP = 1, int MINB = 1, bool M4 = false>
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP = 1, int MINB = 1, bool M4 = false, bool PK = false>
 int launch_wl(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
     using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>;
-    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4>;
+    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4, PK>;
     nsm *= MINB;
     static bool attr = false;
     if (!attr) {
@@ -811,7 +826,7 @@ int sm_count()
 int ie_contract_variants(int precision, int Nz)
 {
     if (precision == 0) return Nz == 32 ? 11 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
-    return Nz == 32 ? 21 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    return Nz == 32 ? 24 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
@@ -872,6 +887,9 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         case 18: return launch_wl<float, 32, 2, 6, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 19: return launch_wl<float, 32, 2, 5, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 20: return launch_wl<float, 32, 1, 8, 6>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 21: return launch_wl<float, 32, 2, 6, 6, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 22: return launch_wl<float, 32, 2, 4, 6, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 23: return launch_wl<float, 32, 4, 4, 6, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         default: return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
         }
     case 48:
@@ -885,7 +903,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 14 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 16 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -913,6 +931,8 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         if (v == 11) return launch_wl<float, 32, 2, 4, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 12) return launch_wl<float, 32, 2, 5, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 13) return launch_wl<float, 32, 2, 3, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 14) return launch_wl<float, 32, 2, 4, 5, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 15) return launch_wl<float, 32, 2, 5, 5, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 32, 4, 2, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);

@@ -5,7 +5,7 @@
 Builds the operator on the GPU (Green's tensor over the 3-layer background, spectral transform),
 sets a seeded Gaussian-random-field anomaly and runs `--reps` applies in the requested precision
 (0 = complex128, 1 = complex64) on the operator's stream, then prints the CUDA-event time per apply.
-A profiler selects the apply kernels by name (k_fx, k_fy, k_contract_tma, k_by, k_bx).
+A profiler selects the apply kernels by name (k_fx, k_fy, k_contract_tma or k_contract_wl, k_by, k_bx).
 """
 from __future__ import annotations
 
