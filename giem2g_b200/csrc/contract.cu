@@ -7,8 +7,9 @@
 //
 // Design (persistent, one CTA per SM):
 //   * producer warp: one lane streams B units of tensor + their 4-point spectra per stage into shared
-//     memory with cp.async.bulk (TMA engine), tensor with an L2 evict_first hint so the spectra that
-//     neighbouring kernels reuse stay in L2; NSTAGE-deep mbarrier ring;
+//     memory with cp.async.bulk (TMA engine), tensor with an L2 evict_first hint so that it does not
+//     push the spectra and the Krylov vectors out of L2 (the spectra get no hint: pinning them with
+//     evict_last cost the solver's vector kernels their L2 hits); NSTAGE-deep mbarrier ring;
 //   * consumer warps: thread (b, s, z) owns row z of unit b for all 3 components and 4 points and sums
 //     over the j-slice s; complex products use 3 real multiplies (T1=a c, T2=b d, T3=(a+b)(c+d);
 //     re=T1-T2, im=T3-T1-T2), 25% fewer FMAs than 4-multiply complex arithmetic, which matters because
@@ -110,7 +111,7 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
         // ------------------------------- producer warp -------------------------------
         if (tid == Cfg::NC) {
             const uint64_t pol_t = l2_policy_evict_first();
-            const uint64_t pol_u = l2_policy_evict_last();
+            const uint64_t pol_u = l2_policy_evict_normal();
             long long issued = 0;
             bool ok = true;
             for (long long it = 0; it < my_n; it++) {
@@ -375,7 +376,7 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
         // producer warp: one lane streams units (tensor + 4-point spectra) into the stage ring in order
         if (tid == Cfg::NC) {
             const uint64_t pol_t = l2_policy_evict_first();
-            const uint64_t pol_u = l2_policy_evict_last();
+            const uint64_t pol_u = l2_policy_evict_normal();
             long long issued = 0;
             bool ok = true;
             for (long long it = 0; it < my_n; it++) {
@@ -587,7 +588,7 @@ __global__ void __launch_bounds__(CfgW<NZ, S, B, NSTAGE, NP, MINB>::NTHREADS, MI
         // producer warp: one lane streams tensor units and their spectra into the stage ring
         if (tid == Cfg::NC) {
             const uint64_t pol_t = l2_policy_evict_first();
-            const uint64_t pol_u = l2_policy_evict_last();
+            const uint64_t pol_u = l2_policy_evict_normal();
             long long issued = 0;
             bool ok = true;
             for (long long it = 0; it < my_n; it++) {

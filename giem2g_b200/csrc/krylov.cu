@@ -1019,14 +1019,20 @@ struct BatchWork {
     std::vector<KrylovWork *> k;
     std::vector<BatchGroup> groups;
     int *d_active = nullptr;
-    std::vector<int> h_active, dev_active, graph_active;  // host mask, copy on the device, mask of the graph
+    std::vector<int> h_active, dev_active;  // host mask and its copy on the device
     double2 *d_stage = nullptr;  // host-array solves: E_bkg[n] then E_sol[n] (complex128)
     cudaStream_t st = nullptr;
-    cudaGraphExec_t inner_exec = nullptr;
+    // One captured inner cycle per mask of active instances: a solve changes the mask as instances
+    // converge, and the next solve starts from all-active again, so the graphs are kept, not re-captured.
+    struct InnerGraph {
+        std::vector<int> mask;
+        cudaGraphExec_t exec = nullptr;
+        int uses = 0, launches = 0;
+        std::vector<int> applies;
+    };
+    std::vector<InnerGraph> graphs;
     double inner_tol = -1.0;
-    int inner_uses = 0, inner_graph_launches = 0;
-    std::vector<int> inner_graph_applies;
-    std::vector<long long> cv;
+    std::vector<long long> cv;  // operators' configuration generations the graphs were captured with
     std::vector<std::vector<double>> history;
 };
 
@@ -1034,7 +1040,8 @@ static void batch_destroy(BatchWork *b)
 {
     if (!b) return;
     if (b->st) cudaStreamSynchronize(b->st);
-    if (b->inner_exec) cudaGraphExecDestroy(b->inner_exec);
+    for (auto &gr : b->graphs)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
     for (KrylovWork *k : b->k) kw_free(k);
     if (b->d_active) cudaFree(b->d_active);
     if (b->d_stage) cudaFree(b->d_stage);
@@ -1075,7 +1082,6 @@ int batch_create(IeOp *const *ops, int n, int mo, int mi, int precision, void **
     if (cudaMalloc(&b->d_active, sizeof(int) * n) != cudaSuccess) { batch_destroy(b); return G2_ERR_NOMEM; }
     b->h_active.assign(n, 1);
     b->dev_active.assign(n, -1);
-    b->inner_graph_applies.assign(n, 0);
     b->history.resize(n);
     *out = b;
     return G2_OK;
@@ -1198,25 +1204,42 @@ static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
     std::vector<long long> cv;
     for (IeOp *op : b->ops) cv.push_back(op->config_gen);
     const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
-    const bool graphs = !(ng && ng[0] == '1');
-    if (b->inner_exec && (b->inner_tol != tol || b->cv != cv || b->graph_active != b->h_active)) {
-        cudaGraphExecDestroy(b->inner_exec);
-        b->inner_exec = nullptr;
-        b->inner_uses = 0;
+    const bool use_graphs = !(ng && ng[0] == '1');
+    if (b->inner_tol != tol || b->cv != cv) {  // the captured arguments are stale: drop every graph
+        for (auto &gr : b->graphs)
+            if (gr.exec) cudaGraphExecDestroy(gr.exec);
+        b->graphs.clear();
+        b->inner_tol = tol;
+        b->cv = cv;
+    }
+    BatchWork::InnerGraph *gr = nullptr;
+    for (auto &e : b->graphs)
+        if (e.mask == b->h_active) gr = &e;
+    if (!gr) {
+        constexpr size_t kMaxGraphs = 32;
+        if (b->graphs.size() >= kMaxGraphs) {  // oldest first
+            if (b->graphs.front().exec) cudaGraphExecDestroy(b->graphs.front().exec);
+            b->graphs.erase(b->graphs.begin());
+        }
+        b->graphs.emplace_back();
+        gr = &b->graphs.back();
+        gr->mask = b->h_active;
+        gr->applies.assign(b->n, 0);
     }
     auto credit = [&]() {
-        g2_count_launches(b->inner_graph_launches);
+        g2_count_launches(gr->launches);
         for (int i = 0; i < b->n; i++) {
-            if (sizeof(CI) == sizeof(float2)) b->k[i]->applies32 += b->inner_graph_applies[i];
-            else b->k[i]->applies64 += b->inner_graph_applies[i];
+            if (sizeof(CI) == sizeof(float2)) b->k[i]->applies32 += gr->applies[i];
+            else b->k[i]->applies64 += gr->applies[i];
         }
     };
-    if (b->inner_exec) {
-        G2_CUDA_CHECK(cudaGraphLaunch(b->inner_exec, st));
+    if (gr->exec) {
+        G2_CUDA_CHECK(cudaGraphLaunch(gr->exec, st));
         credit();
         return G2_OK;
     }
-    if (!graphs || b->inner_uses++ == 0) return batch_inner<CI>(b, tol, st);
+    // first use of a mask runs eagerly (it may allocate pair scratch, which a capture cannot)
+    if (!use_graphs || gr->uses++ == 0) return batch_inner<CI>(b, tol, st);
     std::vector<int> a0(b->n);
     for (int i = 0; i < b->n; i++) a0[i] = b->k[i]->applies32 + b->k[i]->applies64;
     const long long l0 = g2_launch_total();
@@ -1229,24 +1252,21 @@ static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
         g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
         return G2_ERR_CUDA;
     }
-    b->inner_graph_launches = (int)(g2_launch_total() - l0);
+    gr->launches = (int)(g2_launch_total() - l0);
     for (int i = 0; i < b->n; i++) {
         KrylovWork *k = b->k[i];
-        b->inner_graph_applies[i] = k->applies32 + k->applies64 - a0[i];
-        if (sizeof(CI) == sizeof(float2)) k->applies32 -= b->inner_graph_applies[i];
-        else k->applies64 -= b->inner_graph_applies[i];
+        gr->applies[i] = k->applies32 + k->applies64 - a0[i];
+        if (sizeof(CI) == sizeof(float2)) k->applies32 -= gr->applies[i];
+        else k->applies64 -= gr->applies[i];
     }
-    ce = cudaGraphInstantiate(&b->inner_exec, graph, 0);
+    ce = cudaGraphInstantiate(&gr->exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ce != cudaSuccess) {
         g2_set_error(__FILE__, __LINE__, cudaGetErrorString(ce));
-        b->inner_exec = nullptr;
+        gr->exec = nullptr;
         return G2_ERR_CUDA;
     }
-    b->inner_tol = tol;
-    b->cv = cv;
-    b->graph_active = b->h_active;
-    G2_CUDA_CHECK(cudaGraphLaunch(b->inner_exec, st));
+    G2_CUDA_CHECK(cudaGraphLaunch(gr->exec, st));
     credit();
     return G2_OK;
 }
