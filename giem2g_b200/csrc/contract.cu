@@ -826,8 +826,8 @@ int sm_count()
 // on the operator's own buffers and stores its pick in the operator.
 int ie_contract_variants(int precision, int Nz)
 {
-    if (precision == 0) return Nz == 32 ? 11 : (Nz == 8 || Nz == 16 || Nz == 48 ? 1 : 0);
-    return Nz == 32 ? 24 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    if (precision == 0) return Nz == 32 ? 11 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    return Nz == 32 ? 24 : (Nz == 8 || Nz == 16 || Nz == 48 ? 4 : 0);
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
@@ -836,9 +836,15 @@ int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, 
 {
     const int n = sm_count();
     switch (Nz) {
-    case 8: return launch_cfg<double, 8, 2, 8, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
-    case 16: return launch_cfg<double, 16, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
-    case 48: return launch_cfg<double, 48, 4, 1, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 8:
+        if (v == 1) return launch_wl<double, 8, 4, 8, 16>(G, Uhat, Nx, Ny, err, n, st, gate);
+        return launch_cfg<double, 8, 2, 8, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 16:
+        if (v == 1) return launch_wl<double, 16, 4, 4, 8>(G, Uhat, Nx, Ny, err, n, st, gate);
+        return launch_cfg<double, 16, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+    case 48:
+        if (v == 1) return launch_wl<double, 48, 4, 1, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
+        return launch_cfg<double, 48, 4, 1, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 32:
         if (v == 1) return launch_cfg<double, 32, 4, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 2) return launch_cfg<double, 32, 4, 1, 1, 1, false, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
@@ -862,9 +868,13 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
     switch (Nz) {
     case 8:
         if (v == 1) return launch_w32<8, 2, 16, 3, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 2) return launch_wl<float, 8, 4, 8, 16>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 3) return launch_wl<float, 8, 4, 8, 16, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 8, 2, 16, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 16:
         if (v == 1) return launch_w32<16, 4, 4, 4, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 2) return launch_wl<float, 16, 2, 8, 8>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 3) return launch_wl<float, 16, 2, 8, 8, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 16, 4, 4, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 32:
         switch (v) {
@@ -895,6 +905,8 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         }
     case 48:
         if (v == 1) return launch_w32<48, 4, 1, 2, 1>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 2) return launch_wl<float, 48, 4, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 3) return launch_wl<float, 48, 4, 2, 2, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 48, 4, 1, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
     }
@@ -904,7 +916,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 16 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 3 : 0); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 16 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 4 : 0); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -913,10 +925,12 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
     case 8:
         if (v == 1) return launch_cfg<float, 8, 1, 16, 3, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 2) return launch_w32<8, 1, 16, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 3) return launch_wl<float, 8, 4, 8, 16, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 8, 1, 16, 3, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 16:
         if (v == 1) return launch_cfg<float, 16, 2, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 2) return launch_w32<16, 2, 4, 4, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 3) return launch_wl<float, 16, 2, 4, 8, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 16, 2, 4, 4, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 32:
         if (v == 1) return launch_cfg<float, 32, 4, 1, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
@@ -938,6 +952,7 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 2) return launch_w32<48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 3) return launch_wl<float, 48, 4, 1, 2, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 48, 4, 1, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
     }
