@@ -212,10 +212,9 @@ G2_D void reduce_partials(const double2 *part, int nb, int K, double2 *h, double
 
 // first CGS pass of Arnoldi step j = K-1: h = V^H w, then H(0..j, j) = h, hpass = h
 template <typename C, int K>
-__global__ void __launch_bounds__(kVT) k_dots_first_t(const C *__restrict__ V, size_t ld, const C *__restrict__ w,
-                                                      size_t N, double2 *part, Level L, const int *gate)
+G2_D void dots_first_body(const C *__restrict__ V, size_t ld, const C *__restrict__ w, size_t N, double2 *part,
+                          Level &L)
 {
-    if (gate && *gate == 0) return;
     using R = typename RealOf<C>::T;
     R ax[K + 1], ay[K + 1];
 #pragma unroll
@@ -235,13 +234,40 @@ __global__ void __launch_bounds__(kVT) k_dots_first_t(const C *__restrict__ V, s
     reduce_partials(part, gridDim.x, K, hs, nullptr);
     if (threadIdx.x == 0) cgs_first_body(L, K - 1, hs);
 }
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_dots_first_t(const C *__restrict__ V, size_t ld, const C *__restrict__ w,
+                                                      size_t N, double2 *part, Level L, const int *gate)
+{
+    if (gate && *gate == 0) return;
+    dots_first_body<C, K>(V, ld, w, N, part, L);
+}
+
+// Several instances of one batch in one launch (blockIdx.y = instance): the same blocks, partials,
+// counters and last-block steps per instance as separate launches, so the results are the same; what
+// goes is the launch per instance and its ramp and tail.
+constexpr int KMI = 4;
+template <typename C>
+struct Multi {
+    C *V[KMI];
+    C *w[KMI];
+    double2 *part[KMI];
+    Level L[KMI];
+    const int *gate[KMI];
+};
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_dots_first_m(Multi<C> mm, size_t ld, size_t N)
+{
+    const int y = blockIdx.y;
+    if (mm.gate[y] && *mm.gate[y] == 0) return;
+    Level L = mm.L[y];
+    dots_first_body<C, K>(mm.V[y], ld, mm.w[y], N, mm.part[y], L);
+}
 
 // CGS pass p of step j = K-1: w -= V hpass; dots of the new w; then the pass decision (gmres.F90:277-280)
 template <typename C, int K>
-__global__ void __launch_bounds__(kVT) k_cgs_pass_fused_t(const C *__restrict__ V, size_t ld, C *__restrict__ w,
-                                                          size_t N, double2 *part, Level L, int p, const int *gate)
+G2_D void cgs_pass_body(const C *__restrict__ V, size_t ld, C *__restrict__ w, size_t N, double2 *part, Level &L,
+                        int p)
 {
-    if ((gate && *gate == 0) || L.flags[F_PASS] == 0) return;
     using R = typename RealOf<C>::T;
     constexpr int KA = K > 0 ? K : 1;
     __shared__ double2 hsh[KA];
@@ -280,6 +306,21 @@ __global__ void __launch_bounds__(kVT) k_cgs_pass_fused_t(const C *__restrict__ 
         cgs_next_body(L, K - 1, p);
     }
 }
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_cgs_pass_fused_t(const C *__restrict__ V, size_t ld, C *__restrict__ w,
+                                                          size_t N, double2 *part, Level L, int p, const int *gate)
+{
+    if ((gate && *gate == 0) || L.flags[F_PASS] == 0) return;
+    cgs_pass_body<C, K>(V, ld, w, N, part, L, p);
+}
+template <typename C, int K>
+__global__ void __launch_bounds__(kVT) k_cgs_pass_fused_m(Multi<C> mm, size_t ld, size_t N, int p)
+{
+    const int y = blockIdx.y;
+    if ((mm.gate[y] && *mm.gate[y] == 0) || mm.L[y].flags[F_PASS] == 0) return;
+    Level L = mm.L[y];
+    cgs_pass_body<C, K>(mm.V[y], ld, mm.w[y], N, mm.part[y], L, p);
+}
 
 // ||w||^2 into *nrm2
 template <typename C>
@@ -302,10 +343,8 @@ __global__ void __launch_bounds__(kVT) k_norm2_fused(const C *__restrict__ w, si
 
 // end of Arnoldi step j: V_{j+1} = w / ||w||, then the last block runs the Givens/misfit step
 template <typename C>
-__global__ void __launch_bounds__(kVT) k_scale_finish(C *v, const C *w, size_t N, Level L, int j, double tol,
-                                                      const int *gate)
+G2_D void scale_finish_body(C *v, const C *w, size_t N, Level &L, int j, double tol)
 {
-    if (gate && *gate == 0) return;
     const double inv = 1.0 / L.scal[S_DNORMW];
     // kILP independent elements per thread and iteration, loads first: more bytes in flight per SM
     const size_t S = (size_t)gridDim.x * kVT;
@@ -323,6 +362,22 @@ __global__ void __launch_bounds__(kVT) k_scale_finish(C *v, const C *w, size_t N
     }
     if (!last_block(L.counter)) return;
     if (threadIdx.x == 0) arnoldi_finish_body(L, j, tol);
+}
+template <typename C>
+__global__ void __launch_bounds__(kVT) k_scale_finish(C *v, const C *w, size_t N, Level L, int j, double tol,
+                                                      const int *gate)
+{
+    if (gate && *gate == 0) return;
+    scale_finish_body<C>(v, w, N, L, j, tol);
+}
+// Multi: V[y] is the instance's basis, column j+1 is written
+template <typename C>
+__global__ void __launch_bounds__(kVT) k_scale_finish_m(Multi<C> mm, size_t N, int j, double tol)
+{
+    const int y = blockIdx.y;
+    if (mm.gate[y] && *mm.gate[y] == 0) return;
+    Level L = mm.L[y];
+    scale_finish_body<C>(mm.V[y] + (size_t)(j + 1) * N, mm.w[y], N, L, j, tol);
 }
 
 // ConstructCurrentSolution's triangular solve (gmres.F90:441-445): y = H(0:L,0:L)^-1 g
@@ -680,6 +735,36 @@ template <typename C>
 static void arnoldi_tail(KrylovWork *k, Level &L, C *V, int j, const C *w, double tol, const int *gate, cudaStream_t st)
 {
     k_scale_finish<C><<<vec_grid(k->N), kVT, 0, st>>>(V + (size_t)(j + 1) * k->N, w, k->N, L, j, tol, gate);
+    g2_count_launches(1);
+}
+
+// the same CGS and Arnoldi tail for n lockstep instances (vector length N, nparts blocks each) in one
+// launch per kernel
+template <typename C, int K>
+static void launch_dots_first_km(const Multi<C> &mm, int n, size_t N, int nparts, cudaStream_t st)
+{
+    k_dots_first_m<C, K><<<dim3(nparts, n), kVT, 0, st>>>(mm, N, N);
+}
+template <typename C, int K>
+static void launch_pass_fused_km(const Multi<C> &mm, int n, size_t N, int nparts, int p, cudaStream_t st)
+{
+    k_cgs_pass_fused_m<C, K><<<dim3(nparts, n), kVT, 0, st>>>(mm, N, N, p);
+}
+template <typename C>
+static void cgs_multi(const Multi<C> &mm, int n, size_t N, int nparts, int j, cudaStream_t st)
+{
+    const int K = j + 1;
+    G2_KCASES(launch_dots_first_km, mm, n, N, nparts, st)
+    g2_count_launches(1);
+    for (int p = 1; p <= N_IGS + 1; p++) {
+        G2_KCASES(launch_pass_fused_km, mm, n, N, nparts, p, st)
+        g2_count_launches(1);
+    }
+}
+template <typename C>
+static void arnoldi_tail_multi(const Multi<C> &mm, int n, size_t N, int j, double tol, cudaStream_t st)
+{
+    k_scale_finish_m<C><<<dim3(vec_grid(N), n), kVT, 0, st>>>(mm, N, j, tol);
     g2_count_launches(1);
 }
 
@@ -1168,15 +1253,35 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         auto vj = [&](int i) { return reinterpret_cast<const CI *>(b->k[i]->Vi) + (size_t)j * b->k[i]->N; };
         auto wi = [&](int i) { return reinterpret_cast<CI *>(b->k[i]->wi); };
         if ((rc = batch_apply<CI>(b, vj, wi, F_KRYLOV, st))) return rc;
-        for (int i = 0; i < n; i++) {
-            if (!b->h_active[i]) continue;
-            KrylovWork *k = b->k[i];
-            Level &L = k->Li;
-            const int g = vec_grid(k->N);
-            const int *krylov = L.flags + F_KRYLOV;
-            CI *Vi = reinterpret_cast<CI *>(k->Vi);
-            cgs<CI>(k, L, Vi, j, reinterpret_cast<CI *>(k->wi), krylov, st);
-            arnoldi_tail<CI>(k, L, Vi, j, reinterpret_cast<const CI *>(k->wi), tol, krylov, st);
+        // Arnoldi step j of every active instance: runs of up to KMI instances with the same vector
+        // length share each launch (each instance keeps its own blocks, partials and gates)
+        std::vector<int> act;
+        for (int i = 0; i < n; i++)
+            if (b->h_active[i]) act.push_back(i);
+        for (size_t c = 0; c < act.size();) {
+            KrylovWork *k0 = b->k[act[c]];
+            size_t e = c + 1;
+            while (e < act.size() && e - c < (size_t)KMI && b->k[act[e]]->N == k0->N && b->k[act[e]]->nparts == k0->nparts)
+                e++;
+            if (e - c == 1) {
+                Level &L = k0->Li;
+                CI *Vi = reinterpret_cast<CI *>(k0->Vi);
+                cgs<CI>(k0, L, Vi, j, reinterpret_cast<CI *>(k0->wi), L.flags + F_KRYLOV, st);
+                arnoldi_tail<CI>(k0, L, Vi, j, reinterpret_cast<const CI *>(k0->wi), tol, L.flags + F_KRYLOV, st);
+            } else {
+                Multi<CI> mm{};
+                for (size_t q = 0; q < e - c; q++) {
+                    KrylovWork *k = b->k[act[c + q]];
+                    mm.V[q] = reinterpret_cast<CI *>(k->Vi);
+                    mm.w[q] = reinterpret_cast<CI *>(k->wi);
+                    mm.part[q] = k->part;
+                    mm.L[q] = k->Li;
+                    mm.gate[q] = k->Li.flags + F_KRYLOV;
+                }
+                cgs_multi<CI>(mm, (int)(e - c), k0->N, k0->nparts, j, st);
+                arnoldi_tail_multi<CI>(mm, (int)(e - c), k0->N, j, tol, st);
+            }
+            c = e;
         }
     }
     for (int i = 0; i < n; i++) {
