@@ -1,5 +1,5 @@
 // mbarrier + 1-D bulk-copy (TMA engine) helpers for sm_100a, with bounded waits.
-// No cluster multicast is used anywhere in this library.
+// Every bulk copy here lands in the issuing CTA's own shared memory only.
 #pragma once
 #include <cstdint>
 #include "common.cuh"
