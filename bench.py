@@ -513,7 +513,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variants", default=None,
-                    help="pin the tile shapes instead of autotuning: v64,v32,vpair[,fft_lines] (for profilers)")
+                    help="pin the tile shapes instead of autotuning: v64,v32,vpair[,fft_lines[,fft_lines64]] "
+                         "(for profilers)")
     args = ap.parse_args()
     rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":

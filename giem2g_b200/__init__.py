@@ -76,7 +76,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_apply_ie_operator_device_static", "giem2g_batch_create", "giem2g_batch_solve_device",
     "giem2g_solve_batched", "giem2g_batch_misfit_history", "giem2g_batch_delete",
     "giem2g_apply_ie_operator_device_batch", "giem2g_gemm_bf16_tn", "giem2g_im2col3d_bf16",
-    "giem2g_col2im3d_f32", "giem2g_set_outer_preconditioner", "giem2g_set_fft_lines",
+    "giem2g_col2im3d_f32", "giem2g_set_outer_preconditioner", "giem2g_set_fft_lines", "giem2g_set_fft_lines_precision",
     "giem2g_set_kernel_timing", "giem2g_last_contract_ms",
     "giem2g_rc_create", "giem2g_rc_receivers", "giem2g_rc_calc_kernel", "giem2g_rc_calc_fft_of_kernel",
     "giem2g_rc_get_kernel", "giem2g_rc_set_anomaly_conductivity", "giem2g_rc_recalculate",
@@ -149,6 +149,7 @@ def lib():
     L.giem2g_col2im3d_f32.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, ip, vp]
     L.giem2g_set_outer_preconditioner.argtypes = [vp, ip, PRECOND_FN, vp]
     L.giem2g_set_fft_lines.argtypes = [vp, ip]
+    L.giem2g_set_fft_lines_precision.argtypes = [vp, ip, ip]
     L.giem2g_set_precision.argtypes = [vp, ip]
     L.giem2g_set_preconditioner.argtypes = [vp, ip, ctypes.c_char_p]
     L.giem2g_preconditioner_calls.argtypes = [vp]
@@ -331,8 +332,11 @@ class IEOperator:
     def preconditioner_calls(self) -> int:
         return int(lib().giem2g_preconditioner_calls(self.handle))
 
-    def set_fft_lines(self, lines: int):
-        _check(lib().giem2g_set_fft_lines(self.handle, lines), "set_fft_lines")
+    def set_fft_lines(self, lines: int, precision: int | None = None):
+        if precision is None:
+            _check(lib().giem2g_set_fft_lines(self.handle, lines), "set_fft_lines")
+        else:
+            _check(lib().giem2g_set_fft_lines_precision(self.handle, precision, lines), "set_fft_lines")
 
     def set_kernel_timing(self, on: bool):
         _check(lib().giem2g_set_kernel_timing(self.handle, 1 if on else 0), "set_kernel_timing")

@@ -65,27 +65,35 @@ def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> di
         op.set_contract_variant(prec, best[0])
         picks[prec] = {"variant": best[0], "ms": best[1], "all_ms": all_ms}
         cache[ck] = picks[prec]
-    # FFT lines per CTA (one setting for both precisions), timed on the paired complex64 apply
+    # FFT lines per CTA, per precision: complex64 timed on the paired apply (the inner solver's), complex128
+    # on the FP64 apply; the shared-memory tile per line doubles with the element size, so they can differ
+    def time_lines(prec, run):
+        best, all_ms = None, []
+        for lines in (32, 16, 8):
+            op.set_fft_lines(lines, precision=prec)
+            for _ in range(2):
+                run()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            all_ms.append(round(ms, 5))
+            if best is None or ms < best[1]:
+                best = (lines, ms)
+        op.set_fft_lines(best[0], precision=prec)
+        return {"lines": best[0], "ms": best[1], "all_ms": all_ms}
+
     x = torch.randn(op.nvec, dtype=torch.complex64, device="cuda")
     x2, y, y2 = torch.randn_like(x), torch.empty_like(x), torch.empty_like(x)
-    best, all_ms = None, []
-    for lines in (32, 16, 8):
-        op.set_fft_lines(lines)
-        for _ in range(2):
-            apply_device_batch(op, [x.data_ptr(), x2.data_ptr()], [y.data_ptr(), y2.data_ptr()], 1)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(reps):
-            apply_device_batch(op, [x.data_ptr(), x2.data_ptr()], [y.data_ptr(), y2.data_ptr()], 1)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        all_ms.append(round(ms, 5))
-        if best is None or ms < best[1]:
-            best = (lines, ms)
-    op.set_fft_lines(best[0])
-    picks["fft_lines"] = {"lines": best[0], "ms": best[1], "all_ms": all_ms}
+    picks["fft_lines"] = time_lines(1, lambda: apply_device_batch(op, [x.data_ptr(), x2.data_ptr()],
+                                                                  [y.data_ptr(), y2.data_ptr()], 1))
+    xd = torch.randn(op.nvec, dtype=torch.complex128, device="cuda")
+    yd = torch.empty_like(xd)
+    picks["fft_lines64"] = time_lines(0, lambda: op.apply_device(xd.data_ptr(), yd.data_ptr(), 0))
     op.check_device_error()
     if cache_path:
         try:
@@ -96,12 +104,12 @@ def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> di
 
 
 def pin_contraction(op, spec: str) -> dict:
-    """Set the tile shapes by hand instead of timing them: spec = "v64,v32,vpair[,fft_lines]" (the
-    variant numbers the tuner reports).  Profilers need it, because timings taken under a profiler pick
-    other shapes than the plain run does."""
+    """Set the tile shapes by hand instead of timing them: spec = "v64,v32,vpair[,fft_lines[,fft_lines64]]"
+    (the numbers the tuner reports; one FFT lines value sets both precisions, a second one complex128's).
+    Profilers need it, because timings taken under a profiler pick other shapes than the plain run does."""
     parts = [int(t) for t in spec.split(",")]
-    if len(parts) not in (3, 4):
-        raise ValueError("expected v64,v32,vpair[,fft_lines]")
+    if len(parts) not in (3, 4, 5):
+        raise ValueError("expected v64,v32,vpair[,fft_lines[,fft_lines64]]")
     picks = {}
     for prec, v in enumerate(parts[:3]):
         if op.contract_variants(prec) > 1:
@@ -109,7 +117,11 @@ def pin_contraction(op, spec: str) -> dict:
                 raise ValueError(f"variant {v} out of range for precision {prec}")
             op.set_contract_variant(prec, v)
         picks[str(prec)] = {"variant": v, "ms": None, "pinned": True}
-    if len(parts) == 4:
+    if len(parts) >= 4:
         op.set_fft_lines(parts[3])
         picks["fft_lines"] = {"lines": parts[3], "ms": None, "pinned": True}
+        picks["fft_lines64"] = {"lines": parts[3], "ms": None, "pinned": True}
+    if len(parts) == 5:
+        op.set_fft_lines(parts[4], precision=0)
+        picks["fft_lines64"] = {"lines": parts[4], "ms": None, "pinned": True}
     return picks

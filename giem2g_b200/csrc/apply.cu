@@ -349,7 +349,7 @@ static void launch_x(bool fwd, IeOp *op, const VecSet<CT<R>> &vs, CT<R> *U1, cud
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = vs.nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
-    const int NL = lines_for(L, es, op->fft_lines), nt = threads_for(L, NL);
+    const int NL = lines_for(L, es, op->fft_lines[es == sizeof(double2) ? 0 : 1]), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
     dim3 grid((ZL + NL - 1) / NL, Ny);
     static bool attr = false;
@@ -366,7 +366,7 @@ static void launch_y(bool fwd, IeOp *op, int nv, CT<R> *U1, CT<R> *Uh, cudaStrea
 {
     const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
-    const int NL = lines_for(L, es, op->fft_lines), nt = threads_for(L, NL);
+    const int NL = lines_for(L, es, op->fft_lines[es == sizeof(double2) ? 0 : 1]), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
     dim3 grid((ZL + NL - 1) / NL, 2 * Nx);
     static bool attr = false;

@@ -465,7 +465,17 @@ int giem2g_set_fft_lines(void *ie, int lines)
     IeOp *op = resolve(ie);
     if (!op || (lines != 4 && lines != 8 && lines != 16 && lines != 32))
         return fail(G2_ERR_ARG, "giem2g_set_fft_lines: lines must be 4, 8, 16 or 32");
-    op->fft_lines = lines;
+    op->fft_lines[0] = op->fft_lines[1] = lines;
+    op->config_gen++;
+    return set_status(0);
+}
+
+int giem2g_set_fft_lines_precision(void *ie, int precision, int lines)
+{
+    IeOp *op = resolve(ie);
+    if (!op || (precision != 0 && precision != 1) || (lines != 4 && lines != 8 && lines != 16 && lines != 32))
+        return fail(G2_ERR_ARG, "giem2g_set_fft_lines_precision: precision 0 or 1, lines 4, 8, 16 or 32");
+    op->fft_lines[precision] = lines;
     op->config_gen++;
     return set_status(0);
 }

@@ -7,8 +7,10 @@
 //           and emits X[k2 + N2*k1].
 // PAD_IN: inputs with index >= L/2 are zero (zero-padded transform) and are neither loaded nor
 // multiplied.  CROP_OUT: only outputs with index < L/2 are produced.
-// Register DFTs are radix-2 decimation-in-frequency with compile-time indexing; every twiddle comes
-// from one table tw[j] = exp(-2 pi i j / L), j < L, held in shared memory.
+// Register DFTs are radix-2 decimation-in-frequency with compile-time indexing; the twiddles come from
+// one table tw[j] = exp(-2 pi i j / L), j < L, held in shared memory, except the factors -i (+i in the
+// inverse), which the register DFTs apply exactly as a swap and a sign (7 of the 17 twiddle products of a
+// 16-point DFT).
 #pragma once
 #include "common.cuh"
 
@@ -30,6 +32,21 @@ G2_D C twid(const C *tw, int idx)
     return w;
 }
 
+// d * W_N^e for the register DFTs: e = 0 is 1 and e = N/4 is -i (forward) or +i (inverse), exactly (a
+// swap and a sign); other exponents read the table.
+template <typename C, int N, bool INV>
+G2_D C twiddle_mul(C d, int e, const C *tw, int Lstride)
+{
+    if (e == 0) return d;
+    if (4 * e == N) {
+        C r;
+        if (INV) { r.x = -d.y; r.y = d.x; }
+        else { r.x = d.y; r.y = -d.x; }
+        return r;
+    }
+    return cmul(d, twid<C, INV>(tw, e * Lstride));
+}
+
 // In-place N-point DFT of a[] (natural order in, bit-reversed order out).  L/N is the table stride.
 // If HALF_ZERO, a[N/2..N-1] are zero on entry (first stage pruned).
 template <typename C, int N, bool INV, bool HALF_ZERO>
@@ -44,12 +61,11 @@ G2_D void reg_dft_dif(C (&a)[N], const C *tw, int Lstride)
                 const C u = a[g + j];
                 if (HALF_ZERO && h == N / 2) {
                     a[g + j] = u;
-                    a[g + j + h] = (j == 0) ? u : cmul(u, twid<C, INV>(tw, j * (N / (2 * h)) * Lstride));
+                    a[g + j + h] = twiddle_mul<C, N, INV>(u, j * (N / (2 * h)), tw, Lstride);
                 } else {
                     const C v = a[g + j + h];
                     a[g + j] = u + v;
-                    const C d = u - v;
-                    a[g + j + h] = (j == 0) ? d : cmul(d, twid<C, INV>(tw, j * (N / (2 * h)) * Lstride));
+                    a[g + j + h] = twiddle_mul<C, N, INV>(u - v, j * (N / (2 * h)), tw, Lstride);
                 }
             }
         }

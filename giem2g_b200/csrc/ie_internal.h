@@ -55,7 +55,7 @@ struct IeOp {
     int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
     bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
     int contract_variant[3] = {0, 0, 0};  // tile-shape variant: FP64, complex64, paired complex64
-    int fft_lines = 32;                   // lines per CTA of the FFT passes (autotuned: 32, 16 or 8)
+    int fft_lines[2] = {32, 32};          // lines per CTA of the FFT passes, complex128 / complex64 (autotuned)
     long long config_gen = 0;             // bumped on every launch-shape change; captured graphs compare it
     // outer right-preconditioner hook (learned preconditioner): 0 off, 1 warm-starts the inner GMRES,
     // 2 replaces it

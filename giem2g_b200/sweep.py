@@ -65,7 +65,8 @@ def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner
         for prec in (0, 1, 2):
             if str(prec) in tuned and op.contract_variants(prec) > 1:
                 op.set_contract_variant(prec, tuned[str(prec)]["variant"])
-        op.set_fft_lines(tuned["fft_lines"]["lines"])
+        op.set_fft_lines(tuned["fft_lines"]["lines"], precision=1)
+        op.set_fft_lines(tuned["fft_lines64"]["lines"], precision=0)
     out["tuned"] = tuned
     inst_ops, d_rhs = [], []
     for mf, op in ops:

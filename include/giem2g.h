@@ -112,8 +112,10 @@ int giem2g_check_device_error(void *ie);
  * (what the autotuner in giem2g_b200.autotune sets after timing them). */
 int giem2g_contract_variants(void *ie, int precision);  /* precision 2: paired complex64 */
 int giem2g_set_contract_variant(void *ie, int precision, int variant);
-/* Lines per CTA of the FFT passes (4, 8, 16 or 32; default 32), also set by the autotuner. */
+/* Lines per CTA of the FFT passes (4, 8, 16 or 32; default 32), also set by the autotuner: for both
+ * precisions, or for one (0 complex128, 1 complex64, the paired apply included). */
 int giem2g_set_fft_lines(void *ie, int lines);
+int giem2g_set_fft_lines_precision(void *ie, int precision, int lines);
 /* Kernel timing: with on != 0, every device apply outside a stream capture records CUDA events around
  * its contraction launch; giem2g_last_contract_ms returns the last one (ms, -1 if none). */
 int giem2g_set_kernel_timing(void *ie, int on);

@@ -13,6 +13,7 @@ class FakeOp:
         self.counts = counts  # precision -> number of variants
         self.set = {}
         self.lines = None
+        self.lines64 = None
 
     def contract_variants(self, prec):
         return self.counts[prec]
@@ -20,8 +21,12 @@ class FakeOp:
     def set_contract_variant(self, prec, v):
         self.set[prec] = v
 
-    def set_fft_lines(self, lines):
-        self.lines = lines
+    def set_fft_lines(self, lines, precision=None):
+        if precision is None:
+            self.lines = lines
+            self.lines64 = lines
+        else:
+            self.lines64 = lines
 
 
 def test_pin_sets_every_precision_and_the_fft_lines():
@@ -44,7 +49,14 @@ def test_pin_skips_precisions_with_a_single_shape():
     assert op.set == {1: 2}
 
 
-@pytest.mark.parametrize("spec", ["5,21", "1,2,3,4,5", "x,1,2"])
+def test_pin_second_fft_lines_value_is_complex128s():
+    op = FakeOp({0: 11, 1: 24, 2: 16})
+    picks = pin_contraction(op, "5,21,14,16,8")
+    assert op.lines == 16 and op.lines64 == 8
+    assert picks["fft_lines"]["lines"] == 16 and picks["fft_lines64"]["lines"] == 8
+
+
+@pytest.mark.parametrize("spec", ["5,21", "1,2,3,4,5,6", "x,1,2"])
 def test_pin_rejects_malformed_specs(spec):
     with pytest.raises(ValueError):
         pin_contraction(FakeOp({0: 11, 1: 24, 2: 16}), spec)
