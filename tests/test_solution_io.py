@@ -83,3 +83,25 @@ def test_receivers_from_input():
     from giem2g_b200.solution_io import receivers_from_input
     z, xs, ys = receivers_from_input({"Recievers": [{"depth": 0, "xshift": 1.5, "yshift": 0}, {"depth": 200.0}]})
     assert z == [0.0, 200.0] and xs == [1.5, 0.0] and ys == [0.0, 0.0]
+
+
+def test_model_from_input(tmp_path):
+    """The driver's model: grid, borders, background truncated to the layer count, frequencies, FGMRES
+    defaults, and a conductivity file named relative to the input's directory."""
+    from giem2g_b200.driver import model_from_input
+    Nx, Ny, Nz = 4, 2, 3
+    (tmp_path / "sig.txt").write_text(" ".join(["1.0D-2"] * (Nx * Ny * Nz)))
+    inp = {
+        "Background": {"Conductivity": [0.0, 0.01, 0.001, 0.1], "Thickness": [500.0, 1500.0, 99.0]},
+        "Anomaly": {"Nx": Nx, "Ny": Ny, "Nz": Nz, "dx": 50.0, "dy": 60.0,
+                    "zborders": [0.0, 25.0, 50.0, 100.0, 999.0], "Conductivity": "sig.txt"},
+        "Frequencies": [0.1, 1, "10"],
+        "FGMRES": {"Tolerance": 1e-6, "OuterBufferSize": 20},
+    }
+    m, sig, freqs, ctl = model_from_input(inp, str(tmp_path))
+    assert (m.Nx, m.Ny, m.Nz) == (Nx, Ny, Nz) and (m.dx, m.dy) == (50.0, 60.0)
+    assert list(m.z) == [0.0, 25.0, 50.0, 100.0]  # Nz + 1 borders
+    assert list(m.thick) == [500.0, 1500.0, 99.0][: len(inp["Background"]["Conductivity"]) - 1]
+    assert freqs == [0.1, 1.0, 10.0] and m.freq == 0.1
+    assert sig.shape == (Ny, Nx, Nz) and np.all(sig == 1e-2)
+    assert ctl == {"outer_buf": 20, "inner_buf": 10, "max_restart": 100, "tol": 1e-6}
