@@ -474,7 +474,8 @@ def run_b200(args, rank, world, local_rank):
                          "traffic": _profiles_traffic(), "kernel": "FP64 IE apply (5 kernels; contraction dominant)",
                          "bytes_per_launch": B64, "ms_per_launch": ms64, "peak_source": peak_src},
             "dominant_kernel": {
-                "kernel": "k_contract_tma (Green's-tensor contraction)",
+                "kernel": "Green's-tensor contraction (k_contract_wl or k_contract_tma: the autotuned shape in "
+                          "config.contract_variants)",
                 "bytes_per_launch_fp64": TB64, "ms_fp64": mc64, "achieved_gbs_fp64": TB64 / (mc64 * 1e-3) / 1e9,
                 "frac_fp64": TB64 / (mc64 * 1e-3) / 1e9 / peak,
                 "bytes_per_launch_c64": TB64 // 2, "ms_c64": mc32, "achieved_gbs_c64": TB64 / 2 / (mc32 * 1e-3) / 1e9,
