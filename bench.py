@@ -13,9 +13,17 @@ Multi-GPU: independent replicas (one process per GPU, no data-path collective); 
 communication is the barrier and the max-over-ranks of the timing.
 
 --impl reference: the reference's CPU path.  The Fortran/MPI/FFTW reference cannot be built on
-this image, so the CPU restatement in oracle/ (FP64, OpenMP on all host cores) is timed instead:
-each step is one outer FGMRES iteration of the 128x128x32 solve (a bounded sample); the solve
-rate follows from the outer-iteration count of the full FP64 solve done once in set-up.
+this image, so the CPU restatement in oracle/ (FP64, OpenMP on all host cores) is timed instead.
+Set-up solves both polarisations in full once (their outer-iteration counts and times).  Each step
+is one outer FGMRES iteration (a bounded sample: the initial residual, 13 applies of the outer
+iteration, the final true residual) of one polarisation, alternating EY and EX; the solve time it
+stands for counts the two residual applies once and the outer iteration n_outer times:
+t_solve = n_outer * (t_sample - 2 t_apply) + 2 t_apply, with t_apply the oracle's apply timed in
+set-up.  The line reports the full solves' own rate beside it.
+
+Profiler workloads (no JSON contract; one line of timings):
+  --apply-only      a few IE applies at a given grid (kernels k_fx, k_fy, contraction, k_by, k_bx)
+  --receivers-only  the receiver-field tensor build and a few recalculations
 """
 from __future__ import annotations
 
@@ -133,8 +141,10 @@ def build_problem():
     return m, sig, e_y, e_x
 
 
-def cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, nthreads):
-    """Time one outer FGMRES iteration of the oracle's FP64 solver (a bounded sample of the solve)."""
+def cpu_solve_estimate(m, sig, sh, ah, n_outer, nthreads):
+    """One outer FGMRES iteration of the oracle's FP64 solver (a bounded sample of the solve: initial residual,
+    one outer iteration, final true residual) and the solve time it stands for, n_outer*(t - 2 t_apply) +
+    2 t_apply, with the oracle's apply timed alongside.  Returns (sample s, apply s, applies, solve s)."""
     import oracle
     from giem2g_b200.synthetic import csiga_from_sigma
     from giem2g_b200.sources import plane_wave_integral
@@ -142,10 +152,24 @@ def cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, nthreads):
     csigb, sqsigb = oracle.background_cells(m)
     E0 = plane_wave_integral(m, 1)
     t = time.perf_counter()
+    for _ in range(2):
+        oracle.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, E0, nthreads=nthreads)
+    t_apply = (time.perf_counter() - t) / 2
+    t = time.perf_counter()
     _, info, _ = oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, E0, None, 1, INNER, 1, TOL,
                               nthreads=nthreads)
     dt = time.perf_counter() - t
-    return dt, info.applies
+    return dt, t_apply, info.applies, n_outer * (dt - 2.0 * t_apply) + 2.0 * t_apply
+
+
+WORKLOAD = ("IE solve 128x128x32 (50x50x25 m cells), 3-layer background, 0.1 Hz, pols EY+EX, nested FGMRES 30/10, "
+            "outer rel.res 1e-6")
+
+
+def _config(world):
+    """The config both arms print: the problem, its parallel layout and the L2 note (nothing arm-specific)."""
+    return {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
+            "l2": "working set > L2 (tensor 545 MB c64 + 1.09 GB c128)"}
 
 
 def run_reference(args, rank, world):
@@ -157,7 +181,7 @@ def run_reference(args, rank, world):
     from giem2g_b200.synthetic import csiga_from_sigma
     oracle.build()
     ncores = os.cpu_count() or 1
-    m, sig, e_y, _ = build_problem()
+    m, sig, e_y, e_x = build_problem()
     t0 = time.perf_counter()
     S, A = oracle.green_tensor(m, nthreads=ncores)
     sh, ah = oracle.tensor_spectrum(m.Nx, m.Ny, m.Nz, S, A, nthreads=ncores)
@@ -165,35 +189,59 @@ def run_reference(args, rank, world):
     t_setup = time.perf_counter() - t0
     csiga = csiga_from_sigma(sig, m.freq)
     csigb, sqsigb = oracle.background_cells(m)
+    # the oracle's apply alone (the two residual applies a sample holds once per solve)
+    v = np.ascontiguousarray(e_y)
+    oracle.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v, nthreads=ncores)
     t0 = time.perf_counter()
-    _, info, hist = oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, e_y, None, OUTER, INNER,
-                                 MAXRESTART, TOL, nthreads=ncores)
-    t_full = time.perf_counter() - t0
-    n_outer = max(1, info.iterations)
-    for _ in range(args.warmup):
-        cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, ncores)
-    times = []
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        dt, _ = cpu_outer_iteration_rate(m, sig, sh, ah, n_outer, ncores)
-        times.append(dt)
-    total = time.perf_counter() - t0
-    per_iter = total / args.steps
-    value = 1.0 / (per_iter * n_outer)
+    for _ in range(3):
+        oracle.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v, nthreads=ncores)
+    t_apply = (time.perf_counter() - t0) / 3
+    # full solves of both polarisations: outer-iteration counts and the true solve times
+    pols = [("EY", e_y), ("EX", e_x)]
+    n_outer, t_full, applies = [], [], []
+    for _, rhs in pols:
+        t0 = time.perf_counter()
+        _, info, _ = oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, rhs, None, OUTER, INNER,
+                                  MAXRESTART, TOL, nthreads=ncores)
+        t_full.append(time.perf_counter() - t0)
+        n_outer.append(max(1, info.iterations))
+        applies.append(info.applies)
+
+    def sample(i):
+        _, rhs = pols[i % 2]
+        t = time.perf_counter()
+        oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, rhs, None, 1, INNER, 1, TOL,
+                     nthreads=ncores)
+        dt = time.perf_counter() - t
+        n = n_outer[i % 2]
+        return dt, n * (dt - 2.0 * t_apply) + 2.0 * t_apply
+
+    for i in range(args.warmup):
+        sample(i)
+    t_solves, samples = 0.0, []
+    for i in range(args.steps):
+        dt, ts = sample(i)
+        samples.append(dt)
+        t_solves += ts
+    value = args.steps / t_solves
+    full_value = len(pols) / sum(t_full)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded GRF conductivity)",
-        "config": {"workload": "IE solve 128x128x32, 3-layer background, 0.1 Hz, pol EY, FGMRES 30/10, "
-                               "outer rel.res 1e-6, FP64",
-                   "step": "one outer FGMRES iteration of the FP64 solve (bounded sample)"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_solves / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded GRF conductivity, plane-wave sources)",
+        "config": _config(world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": ncores, "kind": "port",
-                         "sample": f"{args.steps} outer FGMRES iterations (1 + {INNER}+2 + 1 applies each) of the "
-                                   f"oracle FP64 solver; solve = {n_outer} outer iterations (full solve in set-up: "
-                                   f"{t_full:.1f} s, {info.applies} applies)"},
+                         "sample": f"{args.steps} outer FGMRES iterations, EY and EX alternating (1 + 13 + 1 FP64 "
+                                   f"applies each, mean {np.mean(samples):.2f} s) of the oracle solver on {ncores} "
+                                   f"threads; each stands for one full solve of n_outer = {n_outer} outer "
+                                   f"iterations: n_outer*(sample - 2 t_apply) + 2 t_apply, t_apply = "
+                                   f"{t_apply:.3f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_setup_s": t_setup, "reference_full_solve_s": t_full, "reference_outer_iterations": n_outer,
-        "note": "Fortran/MPI/FFTW reference is not buildable on this image; the CPU restatement (oracle/) is timed",
+        "reference_setup_s": t_setup, "reference_full_solve_s": t_full, "reference_full_solve_value": full_value,
+        "reference_outer_iterations": n_outer, "reference_applies": applies, "reference_apply_s": t_apply,
+        "note": "Fortran/MPI/FFTW reference is not buildable on this image; the CPU restatement (oracle/) is timed. "
+                "precision: complex128 throughout (the reference has no other)",
     }
     print(json.dumps(line))
     return 0
@@ -381,21 +429,25 @@ def run_b200(args, rank, world, local_rank):
 
     ms32_pair = time_pair()
 
-    # the dominant kernel alone: CUDA events around the contraction launch inside eager applies
-    def time_contract(prec, reps=20):
+    # the contraction alone: CUDA events on the operator's stream around its launch inside eager applies
+    # (single FP64, single complex64, and the paired complex64 form the batched step runs)
+    def time_contract(prec, reps=20, pair=False):
         dt = torch.complex128 if prec == 0 else torch.complex64
-        x = torch.randn(n, dtype=dt, device=dev)
-        y = torch.empty_like(x)
+        xs = [torch.randn(n, dtype=dt, device=dev) for _ in range(2 if pair else 1)]
+        ys = [torch.empty_like(x) for x in xs]
         op.set_kernel_timing(True)
         ts = []
         for i in range(reps + 3):
-            op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+            if pair:
+                g2.apply_device_batch(op, [x.data_ptr() for x in xs], [y.data_ptr() for y in ys], 1)
+            else:
+                op.apply_device(xs[0].data_ptr(), ys[0].data_ptr(), prec)
             if i >= 3:
                 ts.append(op.last_contract_ms())
         op.set_kernel_timing(False)
         return float(np.mean(ts))
 
-    mc64, mc32 = time_contract(0), time_contract(1)
+    mc64, mc32, mcp = time_contract(0), time_contract(1), time_contract(1, pair=True)
     B64 = _algorithmic_bytes(m.Nx, m.Ny, m.Nz, 16)
     B32 = _algorithmic_bytes(m.Nx, m.Ny, m.Nz, 8)
     TB64 = 16 * m.Nx * m.Ny * (2 * m.Nz * (m.Nz + 1) + 2 * m.Nz * m.Nz)  # tensor bytes per apply (FP64)
@@ -408,6 +460,13 @@ def run_b200(args, rank, world, local_rank):
         peak = 6650.0
     ach64 = B64 / (ms64 * 1e-3) / 1e9
     ach32 = B32 / (ms32 * 1e-3) / 1e9
+    # paired complex64 contraction: the tensor read once for two vectors, and its FP32 arithmetic counted as
+    # 4-multiply complex multiply-adds (8 flops) -- 9 Nz x Nz blocks at 4 points per (kx, ky) pair, 2 vectors --
+    # against the nominal FP32 FMA peak (148 SMs x 128 lanes x 2 flops x the maximum SM clock)
+    TB32 = TB64 // 2
+    flops_pair = 2 * 8 * 9 * m.Nz * m.Nz * 4 * m.Nx * m.Ny
+    props = torch.cuda.get_device_properties(dev)
+    fp32_peak = props.multi_processor_count * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
 
     # receiver fields (the reference's "Recalculate Fields") for one line of surface receivers on this grid:
     # receiver tensor build + its spectrum (once per frequency) and one recalculation (per solution)
@@ -449,11 +508,13 @@ def run_b200(args, rank, world, local_rank):
             oracle.build()
             sh, ah = op.get_ie_kernel_spectral()
             ncores = os.cpu_count() or 1
-            dt, applies = cpu_outer_iteration_rate(m, sig, sh, ah, iy64b.iterations, ncores)
-            cpu = {"value": 1.0 / (dt * max(1, iy64b.iterations)), "unit": UNIT, "cores": ncores, "kind": "port",
+            n_it = max(1, iy64b.iterations)
+            dt, t_ap, applies, t_solve = cpu_solve_estimate(m, sig, sh, ah, n_it, ncores)
+            cpu = {"value": 1.0 / t_solve, "unit": UNIT, "cores": ncores, "kind": "port",
                    "sample": f"one outer FGMRES iteration ({applies} FP64 applies incl. the initial and final "
-                             f"residual) of the oracle solver at 128x128x32 on {ncores} threads = {dt:.2f} s; "
-                             f"solve = {iy64b.iterations} outer iterations (FP64, tol 1e-6)"}
+                             f"residual) of the oracle solver at 128x128x32 on {ncores} threads = {dt:.2f} s, "
+                             f"apply {t_ap:.3f} s; solve = {n_it} outer iterations (FP64, tol 1e-6): "
+                             f"{n_it}*(sample - 2 apply) + 2 apply = {t_solve:.1f} s"}
         except Exception as exc:  # the CPU baseline is reported, never the target
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": f"failed: {exc}"}
 
@@ -463,10 +524,10 @@ def run_b200(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 outer",
             "data": "synthetic (seeded GRF conductivity, plane-wave sources)",
-            "config": {"workload": "IE solve 128x128x32 (50x50x25 m cells), 3-layer background, 0.1 Hz, "
-                                   "pols EY+EX batched, nested FGMRES 30/10, outer rel.res 1e-6, mixed precision",
-                       "parallelism": f"replicas x{world}", "l2": "working set > L2 (tensor 545 MB c64 + 1.09 GB c128)",
-                       "tensor_build_s": t_tensor, "contract_variants": tuned},
+            "config": _config(world),
+            "setup": {"tensor_build_s": t_tensor, "contract_variants": tuned,
+                      "method": "mixed precision (c64 inner GMRES/FFTs/tensor, c128 outer), both polarisations as "
+                                "one lockstep batch"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * vec_bytes,
                     "d2h_bytes_per_step": 2 * vec_bytes},
             "gpu_launches": launches,
@@ -474,13 +535,19 @@ def run_b200(args, rank, world, local_rank):
                          "traffic": _profiles_traffic(), "kernel": "FP64 IE apply (5 kernels; contraction dominant)",
                          "bytes_per_launch": B64, "ms_per_launch": ms64, "peak_source": peak_src},
             "dominant_kernel": {
-                "kernel": "Green's-tensor contraction (k_contract_wl or k_contract_tma: the autotuned shape in "
-                          "config.contract_variants)",
-                "bytes_per_launch_fp64": TB64, "ms_fp64": mc64, "achieved_gbs_fp64": TB64 / (mc64 * 1e-3) / 1e9,
-                "frac_fp64": TB64 / (mc64 * 1e-3) / 1e9 / peak,
-                "bytes_per_launch_c64": TB64 // 2, "ms_c64": mc32, "achieved_gbs_c64": TB64 / 2 / (mc32 * 1e-3) / 1e9,
-                "frac_c64": TB64 / 2 / (mc32 * 1e-3) / 1e9 / peak,
-                "note": "algorithmic bytes = the tensor read once (T*S); the spectrum in/out is intermediate"},
+                "kernel": "paired complex64 Green's-tensor contraction (two vectors per tensor read; the batched "
+                          "step's inner applies), autotuned shape in setup.contract_variants[2]",
+                "ms": mcp, "bytes_per_launch": TB32, "achieved_gbs": TB32 / (mcp * 1e-3) / 1e9,
+                "frac_hbm": TB32 / (mcp * 1e-3) / 1e9 / peak,
+                "flops_per_launch": flops_pair, "achieved_tflops": flops_pair / (mcp * 1e-3) / 1e12,
+                "fp32_peak_tflops_nominal": fp32_peak,
+                "frac_fp32": flops_pair / (mcp * 1e-3) / 1e12 / fp32_peak,
+                "single_fp64": {"ms": mc64, "bytes": TB64, "achieved_gbs": TB64 / (mc64 * 1e-3) / 1e9,
+                                "frac_hbm": TB64 / (mc64 * 1e-3) / 1e9 / peak},
+                "single_c64": {"ms": mc32, "bytes": TB32, "achieved_gbs": TB32 / (mc32 * 1e-3) / 1e9,
+                               "frac_hbm": TB32 / (mc32 * 1e-3) / 1e9 / peak},
+                "note": "algorithmic bytes = the tensor read once (T*S); the spectrum in/out is intermediate; "
+                        "flops = 4-multiply complex count (the kernels use the 3-multiply form)"},
             "apply_c64": {"ms": ms32, "achieved_gbs": ach32, "frac": ach32 / peak, "bytes": B32},
             "apply_c64_pair": {"ms": ms32_pair, "bytes": B32P, "achieved_gbs": B32P / (ms32_pair * 1e-3) / 1e9,
                                "frac": B32P / (ms32_pair * 1e-3) / 1e9 / peak},
@@ -506,6 +573,96 @@ def run_b200(args, rank, world, local_rank):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------
+def run_apply_only(args):
+    """A few IE applies at one grid on the operator's stream (the workload the apply profiles capture): the
+    seeded random-field model of config_grf (seed 7), the GPU Green's tensor and its spectrum, then
+    `--reps` applies of one vector (or two with --nv 2, the paired complex64 form) after `--warmup` untimed
+    ones.  Prints one line of CUDA-event timings."""
+    import torch
+    import giem2g_b200 as g2
+    from giem2g_b200.synthetic import config_grf
+
+    m, sig = config_grf(args.nx, args.ny or args.nx, args.nz, seed=7)
+    t0 = time.perf_counter()
+    op = g2.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    op.calc_fft_of_ie_kernel()
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t0
+    op.set_anomaly_sigma(sig, m.freq)
+    if args.variant is not None:
+        op.set_contract_variant(2 if args.nv == 2 else args.prec, args.variant)
+    if args.fft_lines is not None:
+        op.set_fft_lines(args.fft_lines)
+    dt = torch.complex128 if args.prec == 0 else torch.complex64
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(op.nvec, dtype=dt, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    x2, y2 = torch.randn_like(x), torch.empty_like(x)
+    stream = torch.cuda.ExternalStream(op.stream)
+
+    def one():
+        if args.nv == 2:
+            g2.apply_device_batch(op, [x.data_ptr(), x2.data_ptr()], [y.data_ptr(), y2.data_ptr()], args.prec)
+        else:
+            op.apply_device(x.data_ptr(), y.data_ptr(), args.prec)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.reps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    op.check_device_error()
+    print(json.dumps({"mode": "apply-only", "grid": [m.Nx, m.Ny, m.Nz], "precision": args.prec, "nv": args.nv,
+                      "reps": args.reps, "ms_per_apply": e0.elapsed_time(e1) / args.reps, "tensor_build_s": t_build}))
+    op.delete()
+    return 0
+
+
+def run_receivers_only(args):
+    """Receiver fields at one grid (the workload the receiver profile captures): the receiver tensor of `--nr`
+    receiver depths on the config_grf model (seed 7), its spectrum, and `--reps` recalculations of a seeded
+    random field after `--warmup` untimed ones.  Prints one line of timings."""
+    import torch
+    import giem2g_b200 as g2
+    from giem2g_b200.synthetic import config_grf
+
+    m, sig = config_grf(args.nx, args.ny or args.nx, args.nz, seed=7)
+    depths = [0.0, float(m.z[-1]) + 50.0, 1000.0, 150.0][: args.nr] + [0.0] * max(0, args.nr - 4)
+    rc = g2.RCOperator.from_model(m, depths)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc.calc_rc_kernel(m.csigma, m.thick, m.omega)
+    t1 = time.perf_counter()
+    rc.calc_fft_of_rc_kernel()
+    t2 = time.perf_counter()
+    rc.set_anomaly_sigma(sig, m.freq)
+    nv = 3 * m.Nx * m.Ny * m.Nz
+    E = torch.randn(nv, dtype=torch.complex128, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1))
+    Ea = torch.empty(3 * m.Nx * m.Ny * args.nr, dtype=torch.complex128, device="cuda")
+    Ha = torch.empty_like(Ea)
+    stream = torch.cuda.ExternalStream(rc.stream)
+    for _ in range(args.warmup):
+        rc.recalculate_device(E.data_ptr(), Ea.data_ptr(), Ha.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.reps):
+        rc.recalculate_device(E.data_ptr(), Ea.data_ptr(), Ha.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"mode": "receivers-only", "grid": [m.Nx, m.Ny, m.Nz], "receivers": args.nr,
+                      "tensor_build_s": t1 - t0, "tensor_fft_s": t2 - t1,
+                      "recalculate_ms": e0.elapsed_time(e1) / max(1, args.reps)}))
+    rc.delete()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -516,7 +673,25 @@ def main():
     ap.add_argument("--variants", default=None,
                     help="pin the tile shapes instead of autotuning: v64,v32,vpair[,fft_lines[,fft_lines64]] "
                          "(for profilers)")
+    prof = ap.add_argument_group("profiler workloads (--apply-only, --receivers-only)")
+    prof.add_argument("--apply-only", action="store_true", help="a few IE applies at one grid")
+    prof.add_argument("--receivers-only", action="store_true", help="receiver tensor and recalculations")
+    prof.add_argument("--nx", type=int, default=128)
+    prof.add_argument("--ny", type=int, default=None)
+    prof.add_argument("--nz", type=int, default=32)
+    prof.add_argument("--prec", type=int, default=0, choices=[0, 1])
+    prof.add_argument("--reps", type=int, default=3)
+    prof.add_argument("--variant", type=int, default=None)
+    prof.add_argument("--nv", type=int, default=1, choices=[1, 2], help="vectors per apply (2: paired complex64)")
+    prof.add_argument("--fft-lines", type=int, default=None, choices=[4, 8, 16, 32])
+    prof.add_argument("--nr", type=int, default=1, help="receiver depths")
     args = ap.parse_args()
+    if args.apply_only:
+        return run_apply_only(args)
+    if args.receivers_only:
+        if args.warmup == ap.get_default("warmup"):
+            args.warmup = 1
+        return run_receivers_only(args)
     rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)

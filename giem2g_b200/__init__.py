@@ -70,7 +70,7 @@ EXPORTED_SYMBOLS = [
     "giem2g_set_logger", "giem2g_print_stats", "giem2g_delete_ie_operator",
     "giem2g_last_status", "giem2g_last_error", "giem2g_set_background", "giem2g_set_ie_kernel_spatial",
     "giem2g_get_ie_kernel_spatial", "giem2g_get_ie_kernel_spectral", "giem2g_apply_ie_operator_device",
-    "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_solve",
+    "giem2g_get_stream", "giem2g_last_apply_ms", "giem2g_last_kernel_launches", "giem2g_apply_count", "giem2g_solve",
     "giem2g_solve_device", "giem2g_get_misfit_history", "giem2g_check_device_error",
     "giem2g_contract_variants", "giem2g_set_contract_variant", "giem2g_kernel_launch_count",
     "giem2g_apply_ie_operator_device_static", "giem2g_batch_create", "giem2g_batch_solve_device",
@@ -127,6 +127,8 @@ def lib():
     L.giem2g_last_apply_ms.argtypes = [vp]
     L.giem2g_last_apply_ms.restype = dp
     L.giem2g_last_kernel_launches.argtypes = [vp]
+    L.giem2g_apply_count.argtypes = [vp]
+    L.giem2g_apply_count.restype = ctypes.c_longlong
     L.giem2g_solve.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
     L.giem2g_solve_device.argtypes = [vp, vp, vp, vp, FgmresCtl, ctypes.POINTER(ResultT)]
     L.giem2g_get_misfit_history.argtypes = [vp, vp, ip]

@@ -618,9 +618,14 @@ int ie_apply_pair32(IeOp *op, const float2 *in0, const float2 *in1, float2 *out0
     VecSet<float2> vs{{in0, in1}, {out0, out1}, 2};
     dispatch_x<float>(true, op, vs, U1, st, nullptr);
     dispatch_y<float>(true, op, 2, U1, Uh, st, nullptr);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    const bool timed = op->time_contract && op->evc0 &&
+                       cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone;
+    if (timed) cudaEventRecord(op->evc0, st);
     const int rc = ie_contract_pair32(op->d_tensor32, Uh, op->Nx, op->Ny, op->Nz, op->d_err, st, nullptr,
                                       op->contract_variant[2]);
     if (rc) return rc;
+    if (timed) cudaEventRecord(op->evc1, st);
     dispatch_y<float>(false, op, 2, U1, Uh, st, nullptr);
     dispatch_x<float>(false, op, vs, U1, st, nullptr);
     g2_count_launches(5);

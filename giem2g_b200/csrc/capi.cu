@@ -319,6 +319,8 @@ int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int
     IeOp *op = resolve(ie);
     int rc = check_ready(op, "giem2g_apply_ie_operator_device");
     if (rc) return rc;
+    if (precision != 0 && precision != 1)
+        return fail(G2_ERR_ARG, "giem2g_apply_ie_operator_device: precision must be 0 or 1");
     cudaEventRecord(op->ev0, op->stream);
     if (precision == 0)
         rc = ie_apply_device64(op, reinterpret_cast<const double2 *>(d_in), reinterpret_cast<double2 *>(d_out), op->stream);
@@ -356,6 +358,7 @@ int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_o
                     "%d, above the static maximum of %zu bytes; use giem2g_apply_ie_operator_device",
                     op->Nx, op->Ny, op->Nz, need, precision, cap);
     unsigned char *b = static_cast<unsigned char *>(base);
+    cudaEventRecord(op->ev0, op->stream);
     if (precision == 0)
         rc = ie_apply_device64_scratch(op, reinterpret_cast<const double2 *>(d_in), reinterpret_cast<double2 *>(d_out),
                                        op->stream, reinterpret_cast<double2 *>(b),
@@ -363,6 +366,9 @@ int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_o
     else
         rc = ie_apply_device32_scratch(op, reinterpret_cast<const float2 *>(d_in), reinterpret_cast<float2 *>(d_out),
                                        op->stream, reinterpret_cast<float2 *>(b), reinterpret_cast<float2 *>(b + off_uh));
+    cudaEventRecord(op->ev1, op->stream);
+    op->last_kernel_launches = ie_kernel_launch_count_apply();
+    op->mult_num++;
     if (rc) return fail(rc, "giem2g_apply_ie_operator_device_static: %s", giem2g_last_error());
     return set_status(0);
 }
@@ -712,6 +718,12 @@ int giem2g_last_kernel_launches(void *ie)
 {
     IeOp *op = resolve(ie);
     return op ? op->last_kernel_launches : 0;
+}
+
+long long giem2g_apply_count(void *ie)
+{
+    IeOp *op = resolve(ie);
+    return op ? op->mult_num : -1;
 }
 
 void giem2g_set_logger(void (*logger)(const char *)) { g_logger = logger; }

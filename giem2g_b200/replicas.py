@@ -3,11 +3,11 @@
 The reference runs one frequency at a time over all MPI ranks and shards the operator in y
 (giem2g.F90:336-373 loops frequencies and polarisations; Distributed_FFT.F90 transposes between
 slabs).  On B200 one instance fits one GPU (128x128x32: 0.55 GB complex64 tensor), so the
-instances themselves are the unit of parallelism: rank r of W takes instances r, r+W, r+2W, ...
-of the row-major (frequency, polarisation) list, builds the Green's tensor of each of its
-frequencies on its own GPU and solves; there is no collective on the data path.  The only
-communication is the barrier around timed regions, the max over ranks of a device time, and the
-final gather of the per-instance results to rank 0.
+frequencies themselves are the unit of parallelism: rank r of W takes frequencies r, r+W, r+2W, ...
+and solves every polarisation of each of them, so the two polarisations of a frequency share one
+Green's tensor build and, in the batched solver, every tensor read of their paired applies.  There
+is no collective on the data path.  The only communication is the barrier around timed regions, the
+max over ranks of a device time, and the final gather of the per-instance results to rank 0.
 """
 from __future__ import annotations
 
@@ -20,10 +20,17 @@ def instances(freqs: Sequence[float], pols: Sequence[int]) -> list[tuple[int, in
 
 
 def shard(n: int, rank: int, world: int) -> list[int]:
-    """Round-robin instance indices owned by `rank` (every index in exactly one rank)."""
+    """Round-robin indices owned by `rank` (every index in exactly one rank)."""
     if world < 1 or not 0 <= rank < world:
         raise ValueError(f"bad rank {rank} of {world}")
     return list(range(rank, n, world))
+
+
+def shard_instances(freqs: Sequence[float], pols: Sequence[int], rank: int, world: int) -> list[tuple[int, int]]:
+    """The (frequency index, polarisation) instances of `rank`: its round-robin share of the frequencies, each
+    with all of its polarisations, in the reference's visiting order."""
+    mine = set(shard(len(freqs), rank, world))
+    return [(fi, p) for fi, p in instances(freqs, pols) if fi in mine]
 
 
 def max_over_ranks(x: float, device=None) -> float:
@@ -41,12 +48,11 @@ def run_sweep(solve_one: Callable[[int, int], object], freqs: Sequence[float], p
               rank: int = 0, world: int = 1) -> dict[tuple[int, int], object] | None:
     """Solve this rank's share of the sweep; rank 0 returns {(fi, pol): result} for all instances.
 
-    `solve_one(fi, pol)` runs one instance on this rank's GPU and returns a picklable result.
-    Frequencies are visited in order so a rank builds each of its tensors once.
+    `solve_one(fi, pol)` runs one instance on this rank's GPU and returns a picklable result.  A rank owns
+    whole frequencies (all polarisations) and visits them in order, so it builds each of its tensors once.
     """
     import torch.distributed as dist
-    todo = instances(freqs, pols)
-    mine = {todo[i]: solve_one(*todo[i]) for i in shard(len(todo), rank, world)}
+    mine = {key: solve_one(*key) for key in shard_instances(freqs, pols, rank, world)}
     if world == 1:
         return mine
     parts = [None] * world if rank == 0 else None

@@ -103,7 +103,9 @@ int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int
  * buffers.  For hosts that must not allocate device memory after start-up.  Grids that need more
  * than 32 MiB of intermediates (18*Nx*Ny*Nz complex of the precision) are rejected with status
  * -1 and a message.  The first call on a device sets up the array's address; make it before any stream
- * capture on that device.  Calls that overlap on the GPU race on the shared array. */
+ * capture on that device (and again after a device reset, which repeats the set-up).  Calls that overlap
+ * on the GPU race on the shared array: each operator has its own stream, so calls on two operators of one
+ * device must be ordered by the host (an event or a synchronisation) even when one thread issues them. */
 int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_out, int precision);
 /* Synchronise the operator's stream and report a device-side error word (bounded waits that ran
  * out) as a nonzero status. */
@@ -125,6 +127,9 @@ void *giem2g_get_stream(void *ie);
 /* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */
 double giem2g_last_apply_ms(void *ie);
 int giem2g_last_kernel_launches(void *ie);
+/* Operator applies since creation or the last giem2g_print_stats (its "Number of matrix-vector
+ * multiplications", Integral_Equation_Module.F90:473-484): every apply entry point and solve counts. */
+long long giem2g_apply_count(void *ie);
 
 /* FGMRES_CTL_TYPE (data_types_module.F90:49-55) */
 typedef struct {

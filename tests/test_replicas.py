@@ -5,7 +5,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from giem2g_b200.replicas import instances, shard
+from giem2g_b200.replicas import instances, shard, shard_instances
 
 
 def test_shard_partitions_instances():
@@ -19,6 +19,22 @@ def test_shard_partitions_instances():
 
 def test_instances_order():
     assert instances([0.1, 1.0], [1, 0]) == [(0, 1), (0, 0), (1, 1), (1, 0)]
+
+
+def test_polarisations_of_a_frequency_stay_on_one_rank():
+    """Sharding is by frequency: EY and EX of one frequency (one tensor build, shared tensor reads in the
+    batched solver) land on the same rank for every world size, and every instance on exactly one rank."""
+    for nf in range(0, 9):
+        freqs = [10.0 ** (k - 3) for k in range(nf)]
+        for w in range(1, 6):
+            owner = {}
+            for r in range(w):
+                for key in shard_instances(freqs, [1, 0], r, w):
+                    assert key not in owner
+                    owner[key] = r
+            assert sorted(owner) == sorted(instances(freqs, [1, 0]))
+            for fi in range(nf):
+                assert owner[(fi, 1)] == owner[(fi, 0)] == fi % w
 
 
 def _free_port():
@@ -63,6 +79,6 @@ def test_two_rank_sweep_gloo():
     assert out[1][0] is None
     assert t0 == 2.0 and out[1][1] == 2.0
     assert sorted(res0) == sorted(instances([0, 1, 2], [1, 0]))
-    for i, key in enumerate(instances([0, 1, 2], [1, 0])):
-        assert res0[key]["rank"] == i % 2
+    for key in instances([0, 1, 2], [1, 0]):
+        assert res0[key]["rank"] == key[0] % 2  # whole frequencies per rank
         assert abs(res0[key]["val"] - [0.01, 0.1, 1.0][key[0]] * (key[1] + 1)) < 1e-15

@@ -33,14 +33,21 @@ def _static(g2, op, x, y, prec):
 
 
 @pytest.mark.parametrize("prec", [0, 1])
-def test_static_apply_matches_device_apply(g2lib, prec):
+def test_static_apply_matches_device_apply(g2lib, orc, prec):
+    """Two calls in a row against the regular device apply and against the oracle's apply of the same
+    spectral tensor; the operator's apply counter counts the static calls too."""
     import torch
     m, sig = config_small_block()
     op = _op(g2lib, m, sig)
+    sh, ah = op.get_ie_kernel_spectral()
+    csiga = csiga_from_sigma(sig, m.freq)
+    csigb, sqsigb = orc.background_cells(m)
     dt = torch.complex128 if prec == 0 else torch.complex64
     tol = TOL64 if prec == 0 else TOL32
-    xs = [torch.from_numpy(random_vec(m, s).ravel()).to("cuda", dt) for s in (11, 12)]
-    for x in xs:  # two calls in a row, different inputs
+    vs = [random_vec(m, s) for s in (11, 12)]
+    n0 = g2lib.lib().giem2g_apply_count(ctypes.c_void_p(op.handle))
+    for v in vs:  # two calls in a row, different inputs
+        x = torch.from_numpy(v.ravel()).to("cuda", dt)
         ref = torch.empty_like(x)
         got = torch.full_like(x, complex(np.nan, np.nan))
         op.apply_device(x.data_ptr(), ref.data_ptr(), prec)
@@ -48,7 +55,11 @@ def test_static_apply_matches_device_apply(g2lib, prec):
         assert rc == 0, g2lib.lib().giem2g_last_error()
         op.check_device_error()
         torch.cuda.synchronize()
-        assert rel(got.cpu().numpy(), ref.cpu().numpy()) < tol
+        got_np = got.cpu().numpy().astype(np.complex128)
+        assert rel(got_np, ref.cpu().numpy().astype(np.complex128)) < tol
+        want = orc.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v)
+        assert rel(got_np.reshape(want.shape), want) < tol
+    assert g2lib.lib().giem2g_apply_count(ctypes.c_void_p(op.handle)) - n0 == 4
     op.delete()
 
 
