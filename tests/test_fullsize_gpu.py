@@ -2,8 +2,9 @@
 background, 0.1 Hz) against the oracle at full size: the Green's tensor at every lag, its spectrum, the apply
 in both precisions, and the solves (the GPU solution put back through the oracle's apply).
 
-Tolerances as on the small grids: tensor 1e-10 relative (cross-layer xx/xy/yy entries bounded at 5 % of the
-block, as in test_green_gpu.py: the anomaly crosses the 500 m interface), spectrum and FP64 apply 1e-12,
+Tolerances as on the small grids: tensor 1e-10 relative, the cross-layer xx/xy/yy entries included (the
+anomaly crosses the 500 m interface; at this model those entries agree to 2e-12, see test_green_c2_gpu.py),
+spectrum and FP64 apply 1e-12,
 complex64 apply 2e-5; the recomputed relative residual of a solve stays within 1.5x the solver's tolerance.
 """
 import numpy as np
@@ -39,8 +40,7 @@ def test_c2_tensor_matches_oracle(c2, orc):
         assert rel(A_g[:, :, c], A_o[:, :, c]) < 1e-10
     for c in range(3):
         assert rel(S_g[:, :, c][..., ~cross], S_o[:, :, c][..., ~cross]) < 1e-10
-        scale = np.abs(S_o[:, :, c]).max()
-        assert np.abs(S_g[:, :, c][..., cross] - S_o[:, :, c][..., cross]).max() < 0.05 * scale
+        assert rel(S_g[:, :, c][..., cross], S_o[:, :, c][..., cross]) < 1e-10
 
 
 def test_c2_spectrum_and_apply_match_oracle(c2, orc):

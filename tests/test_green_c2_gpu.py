@@ -1,13 +1,15 @@
 """The GPU Green's tensor end to end at the benchmark's own size (128x128x32, 50x50x25 m cells, the anomaly
 crossing the 500 m interface at cell 20, 0.1 Hz).
 
-The cross-layer xx/xy/yy entries of the GPU tensor differ from the oracle's by more than the 1e-10 that every
-other entry meets (test_green_gpu.py explains why: the reference arithmetic divides FFT round-off of the VBT
-weights at lambda < 1e-10 /m by lambda).  These tests measure what that difference does downstream: an
+On some small test models the cross-layer xx/xy/yy entries of the GPU tensor differ from the oracle's by more
+than the 1e-10 that every other entry meets (test_green_gpu.py explains why: the reference arithmetic divides
+FFT round-off of the VBT weights at lambda < 1e-10 /m by lambda).  These tests measure that difference at this
+model and what it does downstream: an
 operator built from the ORACLE's spatial tensor (giem2g_set_ie_kernel_spatial) and one built from the GPU's
-(giem2g_calc_ie_kernel) apply the same vector and solve both polarisations in FP64 at tol 1e-8.  The apply
-and the solutions must agree within bounds well below the mixed-precision field error (about 1e-6) that the
-benchmark's method accepts.  The measured figures are printed (pytest -s).
+(giem2g_calc_ie_kernel) apply the same vector and solve both polarisations in FP64 at tol 1e-8.  At this
+model the difference is round-off (2e-12 over the cross-layer entries): the apply agrees to 1e-12 and the
+FP64 solutions to 1e-10, far below the mixed-precision field error (about 1e-6) the benchmark's method
+accepts.  The measured figures are printed (pytest -s).
 """
 import numpy as np
 import pytest
@@ -18,11 +20,13 @@ from tests.helpers import random_vec, rel
 
 pytestmark = pytest.mark.gpu
 
-# bounds on the effect of the cross-layer round-off, relative 2-norms
-APPLY_BOUND = 1e-7
-FIELD_BOUND = 1e-7
-# bound on the cross-layer entries themselves, relative to each component's largest entry
-CROSS_BOUND = 2e-3
+# Measured on a B200 (oracle on 16 host threads): cross-layer entries max |dG| / max|G| 9.9e-15 (xx, yy),
+# 9.1e-17 (xy), 2-norm relative 2.0e-12 over those entries; FP64 apply 1.4e-13; FP64 solutions 4.2e-12 (EY)
+# and 4.1e-12 (EX), 18 outer iterations each.  At this model the cross-layer entries meet the same 1e-10 as
+# every other entry, and the bounds below sit one to two orders of magnitude above the measurement.
+CROSS_BOUND = 1e-10   # 2-norm relative over the cross-layer entries of each of xx, xy, yy
+APPLY_BOUND = 1e-12
+FIELD_BOUND = 1e-10
 
 
 @pytest.fixture(scope="module")
@@ -55,7 +59,7 @@ def test_c2_cross_layer_deviation(two_ops, orc):
         dev = np.abs(S_g[:, :, c][..., cross] - S_o[:, :, c][..., cross]).max() / scale
         blk = rel(S_g[:, :, c][..., cross], S_o[:, :, c][..., cross])
         print(f"cross-layer {name}: max |dG| / max|G| = {dev:.3e}, 2-norm rel over the cross-layer entries {blk:.3e}")
-        worst.append(dev)
+        worst.append(blk)
     assert max(worst) < CROSS_BOUND
 
 
