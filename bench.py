@@ -618,8 +618,10 @@ def run_apply_only(args):
     e1.record(stream)
     torch.cuda.synchronize()
     op.check_device_error()
+    form = 2 if args.nv == 2 else args.prec
     print(json.dumps({"mode": "apply-only", "grid": [m.Nx, m.Ny, m.Nz], "precision": args.prec, "nv": args.nv,
-                      "reps": args.reps, "ms_per_apply": e0.elapsed_time(e1) / args.reps, "tensor_build_s": t_build}))
+                      "variant": args.variant, "variants": op.contract_variants(form), "reps": args.reps,
+                      "ms_per_apply": e0.elapsed_time(e1) / args.reps, "tensor_build_s": t_build}))
     op.delete()
     return 0
 

@@ -311,7 +311,17 @@ template <> struct Bufs<float> {
 
 }  // namespace
 
-int ie_kernel_launch_count_apply() { return 5; }
+static bool uses_ypipe(const IeOp *op, int form)
+{
+    return op->use_fast_contract && op->ypipe_mode[form] >= 0 && ie_ypipe_supported(op->Nx, op->Ny, op->Nz);
+}
+
+int ie_kernel_launch_count_apply(const IeOp *op, int form) { return uses_ypipe(op, form) ? 3 : 5; }
+
+// elements of the spectrum of one vector, and the pipelined pass's counters after it (in 8-byte units, so
+// the same count covers them behind a complex64 or a complex128 spectrum)
+static size_t spectrum_elems(const IeOp *op) { return (size_t)op->Nx * op->Ny * 4 * 3 * op->Nz; }
+static size_t ystate_elems(const IeOp *op) { return (ie_ypipe_state_bytes(op->Nx) + 7) / 8; }
 
 // lines per CTA: tile of at most ~100 KB of shared memory, power of two, <= 32
 static int lines_for(int L, size_t es, int cap)
@@ -417,12 +427,25 @@ static int ie_apply_core(IeOp *op, const CT<R> *d_in, CT<R> *d_out, cudaStream_t
     const CT<R> *G = Bufs<R>::G(op);
     if (!G || !U1 || !Uh) return G2_ERR_STATE;
     VecSet<CT<R>> vs{{d_in, nullptr}, {d_out, nullptr}, 1};
-    dispatch_x<R>(true, op, vs, U1, st, gate);
-    dispatch_y<R>(true, op, 1, U1, Uh, st, gate);
+    const int form = sizeof(R) == 8 ? 0 : 1;
     // contraction (bracketed by events when kernel timing is on; never inside a stream capture)
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     const bool timed = op->time_contract && op->evc0 &&
                        cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone;
+    dispatch_x<R>(true, op, vs, U1, st, gate);
+    if (uses_ypipe(op, form)) {
+        // y-FFT, contraction and inverse y-FFT in one pass, the spectrum as L2-resident scratch
+        int *state = reinterpret_cast<int *>(Uh + spectrum_elems(op));
+        if (timed) cudaEventRecord(op->evc0, st);
+        const int rc = ie_ypipe(op, form, G, U1, Uh, state, st, gate);
+        if (rc) return rc;
+        if (timed) cudaEventRecord(op->evc1, st);
+        dispatch_x<R>(false, op, vs, U1, st, gate);
+        g2_count_launches(3);
+        G2_CUDA_CHECK(cudaGetLastError());
+        return G2_OK;
+    }
+    dispatch_y<R>(true, op, 1, U1, Uh, st, gate);
     if (timed) cudaEventRecord(op->evc0, st);
     int rc_fast = G2_ERR_UNSUPPORTED;
     if (op->use_fast_contract) {
@@ -500,7 +523,7 @@ size_t ie_apply_scratch_elems(const IeOp *op, size_t *n_u1)
 {
     const size_t u1 = (size_t)2 * op->Nx * 3 * op->Nz * op->Ny;
     if (n_u1) *n_u1 = u1;
-    return u1 + (size_t)op->Nx * op->Ny * 4 * 3 * op->Nz;
+    return u1 + spectrum_elems(op) + ystate_elems(op);
 }
 int ie_apply_device64_scratch(IeOp *op, const double2 *d_in, double2 *d_out, cudaStream_t st, double2 *U1,
                               double2 *Uhat)
@@ -528,7 +551,7 @@ static int set_smem_attrs(IeOp *op)
 int ie_alloc_scratch(IeOp *op)
 {
     const size_t n_u1 = (size_t)2 * op->Nx * 3 * op->Nz * op->Ny;
-    const size_t n_uh = (size_t)op->Nx * op->Ny * 4 * 3 * op->Nz;
+    const size_t n_uh = spectrum_elems(op) + ystate_elems(op);
     if (!op->scratch.U1) G2_CUDA_CHECK(cudaMalloc(&op->scratch.U1, n_u1 * sizeof(double2)));
     if (!op->scratch.Uhat) G2_CUDA_CHECK(cudaMalloc(&op->scratch.Uhat, n_uh * sizeof(double2)));
     return set_smem_attrs(op);
@@ -616,11 +639,22 @@ int ie_apply_pair32(IeOp *op, const float2 *in0, const float2 *in1, float2 *out0
     if (!op->use_fast_contract || !ie_contract_pair32_supported(op->Nx, op->Ny, op->Nz)) return G2_ERR_UNSUPPORTED;
     if (!op->d_tensor32 || !U1 || !Uh) return G2_ERR_STATE;
     VecSet<float2> vs{{in0, in1}, {out0, out1}, 2};
-    dispatch_x<float>(true, op, vs, U1, st, nullptr);
-    dispatch_y<float>(true, op, 2, U1, Uh, st, nullptr);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     const bool timed = op->time_contract && op->evc0 &&
                        cudaStreamIsCapturing(st, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone;
+    dispatch_x<float>(true, op, vs, U1, st, nullptr);
+    if (uses_ypipe(op, 2)) {
+        int *state = reinterpret_cast<int *>(Uh + 2 * spectrum_elems(op));
+        if (timed) cudaEventRecord(op->evc0, st);
+        const int rc = ie_ypipe(op, 2, op->d_tensor32, U1, Uh, state, st, nullptr);
+        if (rc) return rc;
+        if (timed) cudaEventRecord(op->evc1, st);
+        dispatch_x<float>(false, op, vs, U1, st, nullptr);
+        g2_count_launches(3);
+        G2_CUDA_CHECK(cudaGetLastError());
+        return G2_OK;
+    }
+    dispatch_y<float>(true, op, 2, U1, Uh, st, nullptr);
     if (timed) cudaEventRecord(op->evc0, st);
     const int rc = ie_contract_pair32(op->d_tensor32, Uh, op->Nx, op->Ny, op->Nz, op->d_err, st, nullptr,
                                       op->contract_variant[2]);

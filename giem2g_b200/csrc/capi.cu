@@ -143,6 +143,8 @@ void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data
     {
         const char *gen = std::getenv("GIEM2G_GENERIC_CONTRACT");
         op->use_fast_contract = !(gen && gen[0] == '1');
+        const char *noy = std::getenv("GIEM2G_NO_YPIPE");
+        if (noy && noy[0] == '1') op->ypipe_mode[0] = op->ypipe_mode[1] = op->ypipe_mode[2] = -1;
     }
     int rc = ie_make_twiddles(op);
     if (!rc) rc = ie_alloc_scratch(op);
@@ -327,7 +329,7 @@ int giem2g_apply_ie_operator_device(void *ie, const void *d_in, void *d_out, int
     else
         rc = ie_apply_device32(op, reinterpret_cast<const float2 *>(d_in), reinterpret_cast<float2 *>(d_out), op->stream);
     cudaEventRecord(op->ev1, op->stream);
-    op->last_kernel_launches = ie_kernel_launch_count_apply();
+    op->last_kernel_launches = ie_kernel_launch_count_apply(op, precision == 0 ? 0 : 1);
     op->mult_num++;
     if (rc) return fail(rc, "giem2g_apply_ie_operator_device: %s", giem2g_last_error());
     return set_status(0);
@@ -367,7 +369,7 @@ int giem2g_apply_ie_operator_device_static(void *ie, const void *d_in, void *d_o
         rc = ie_apply_device32_scratch(op, reinterpret_cast<const float2 *>(d_in), reinterpret_cast<float2 *>(d_out),
                                        op->stream, reinterpret_cast<float2 *>(b), reinterpret_cast<float2 *>(b + off_uh));
     cudaEventRecord(op->ev1, op->stream);
-    op->last_kernel_launches = ie_kernel_launch_count_apply();
+    op->last_kernel_launches = ie_kernel_launch_count_apply(op, precision == 0 ? 0 : 1);
     op->mult_num++;
     if (rc) return fail(rc, "giem2g_apply_ie_operator_device_static: %s", giem2g_last_error());
     return set_status(0);
@@ -438,13 +440,30 @@ static GIEM2G_FGMRES_CTL resolve_precision(const IeOp *op, GIEM2G_FGMRES_CTL ctl
     return ctl;
 }
 
+// Variants [0, n) are the separate-pass contraction shapes (k_fy, contraction, k_by); where the fused pass
+// exists, variants [n, n + ie_ypipe_variants) select it with its own shapes instead.
+static int n_contract(const IeOp *op, int precision)
+{
+    return precision == 2 ? ie_contract_pair_variants(op->Nz) : ie_contract_variants(precision, op->Nz);
+}
+static int n_ypipe(const IeOp *op, int precision)
+{
+    return ie_ypipe_supported(op->Nx, op->Ny, op->Nz) ? ie_ypipe_variants(precision) : 0;
+}
+
 int giem2g_set_contract_variant(void *ie, int precision, int variant)
 {
     IeOp *op = resolve(ie);
     if (!op || precision < 0 || precision > 2) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: bad arguments");
-    const int n = precision == 2 ? ie_contract_pair_variants(op->Nz) : ie_contract_variants(precision, op->Nz);
-    if (variant < 0 || (variant > 0 && variant >= n)) return fail(G2_ERR_ARG, "giem2g_set_contract_variant: variant %d of %d", variant, n);
-    op->contract_variant[precision] = variant;
+    const int n = n_contract(op, precision), ny = n_ypipe(op, precision);
+    if (variant < 0 || (variant > 0 && variant >= n + ny))
+        return fail(G2_ERR_ARG, "giem2g_set_contract_variant: variant %d of %d", variant, n + ny);
+    if (variant >= n && ny > 0) {
+        op->ypipe_mode[precision] = variant - n;
+    } else {
+        op->contract_variant[precision] = variant;
+        op->ypipe_mode[precision] = -1;
+    }
     op->config_gen++;
     return set_status(0);
 }
@@ -489,8 +508,8 @@ int giem2g_set_fft_lines_precision(void *ie, int precision, int lines)
 int giem2g_contract_variants(void *ie, int precision)
 {
     IeOp *op = resolve(ie);
-    if (!op) return 0;
-    return precision == 2 ? ie_contract_pair_variants(op->Nz) : ie_contract_variants(precision, op->Nz);
+    if (!op || precision < 0 || precision > 2) return 0;
+    return n_contract(op, precision) + n_ypipe(op, precision);
 }
 
 int giem2g_check_device_error(void *ie)

@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "ie_internal.h"
 #include "tma.cuh"
+#include "contract_wl.cuh"
 
 namespace {
 
@@ -49,24 +50,6 @@ struct CfgT {
     static_assert(SMEM <= 232448, "exceeds the 227 KB dynamic shared memory of one CTA");
     static_assert(MINB * (SMEM + 1024) <= 233472, "MINB CTAs do not fit the SM's shared memory");
 };
-
-// (a.x*b.x + c.x, a.y*b.y + c.y) in one packed FP32 instruction
-G2_D float2 ffma2(float2 a, float2 b, float2 c)
-{
-    union U { float2 f; unsigned long long u; } ua, ub, uc, ud;
-    ua.f = a;
-    ub.f = b;
-    uc.f = c;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(ud.u) : "l"(ua.u), "l"(ub.u), "l"(uc.u));
-    return ud.f;
-}
-
-template <typename R> struct V2;
-template <> struct V2<double> { using T = double2; };
-template <> struct V2<float> { using T = float2; };
-
-template <int NZ>
-G2_D int sym_idx(int i, int j) { return i <= j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2; }
 
 // NP > 1: NP vectors share every tensor unit (several right-hand sides of one operator); the spectrum of
 // a unit is [slot][vector][3Nz] and point pt = slot * NP + vector.  SPLIT: each thread computes the 4
@@ -308,39 +291,6 @@ struct CfgL {
     static_assert(MINB * (SMEM + 1024) <= 233472, "MINB CTAs do not fit the SM's shared memory");
 };
 
-// one halving step over lane bit B of the slice index, then the next; v[0, LEN) is still held
-template <int B, int LEN, int ZW, int SL, int NR, typename R>
-G2_D void halve_slices(R (&v)[NR], int s, int &f0)
-{
-    if constexpr ((1 << B) < SL) {
-        constexpr int HALF = LEN / 2;
-        const bool up = (s >> B) & 1;
-#pragma unroll
-        for (int i = 0; i < HALF; i++) {
-            const R send = up ? v[i] : v[HALF + i];
-            const R keep = up ? v[HALF + i] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, ZW << B);
-        }
-        if (up) f0 += HALF;
-        halve_slices<B + 1, HALF, ZW, SL, NR>(v, s, f0);
-    }
-}
-
-// Spin (bounded, 2 s) until ticket it-1 has been passed.
-G2_D bool wait_ticket(const int *passed, int it, int *err)
-{
-    const volatile int *p = passed;
-    if (*p >= it) return true;
-    const uint64_t t0 = globaltimer_ns();
-    while (*p < it) {
-        if (globaltimer_ns() - t0 > 2000000000ull) {
-            atomicCAS(err, 0, 17);
-            return false;
-        }
-    }
-    return true;
-}
-
 // PK (complex64): the packed 3-multiply form of k_contract_tma, two instructions per complex multiply-add.
 template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4, bool PK>
 __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREADS, MINB)
@@ -349,9 +299,8 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
 {
     if (gate && *gate == 0) return;  // uniform across the CTA: nothing has been issued yet
     using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>;
-    constexpr int PTS = Cfg::PTS, ZW = Cfg::ZW, W = Cfg::W, P = Cfg::P;
+    constexpr int PTS = Cfg::PTS, ZW = Cfg::ZW, W = Cfg::W;
     using C2 = typename V2<R>::T;
-    constexpr int AW = sizeof(R) == 8 ? asw_width64(NZ) : asw_width32(NZ);
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *stages = smem;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + NSTAGE * Cfg::STAGE_BYTES);
@@ -414,106 +363,13 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
         const unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
         const C2 *gb = reinterpret_cast<const C2 *>(st);
         const C2 *ub = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);  // [pt][c][j]
-        static_assert(!PK || (sizeof(R) == 4 && !M4), "packed pairs are a complex64 3-multiply form");
-        constexpr int NA = M4 ? 2 : 3;
-        R acc[3][PTS][NA];
-        C2 accp[3][PTS];  // PK: (t1, t2) of the 3-multiply form
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int p = 0; p < PTS; p++) {
-                accp[c][p] = C2{R(0), R(0)};
-#pragma unroll
-                for (int k = 0; k < NA; k++) acc[c][p][k] = R(0);
-            }
-        const C2 *gxx = gb, *gxy = gb + P, *gyy = gb + 2 * P, *gzz = gb + 3 * P;
-        const C2 *gxz = gb + 4 * P, *gyz = gb + 4 * P + NZ * NZ;
-#pragma unroll 2
-        for (int jj = 0; jj < Cfg::JS; jj++) {
-            const int j = jj * SL + s;
-            const int si = sym_idx<NZ>(z, j);
-            const int a_zj = asw(z, j, NZ, AW), a_jz = asw(j, z, NZ, AW);
-            const C2 e[8] = {gxx[si], gxy[si], gyy[si], gzz[si], gxz[a_zj], gyz[a_zj], gxz[a_jz], gyz[a_jz]};
-            C2 en[8];  // PK: negated copies (only the ones a negative sign uses survive compilation)
-#pragma unroll
-            for (int k = 0; k < 8; k++) en[k] = C2{-e[k].x, -e[k].y};
-            C2 u[PTS][3];
-            R ue[PTS][3];
-#pragma unroll
-            for (int p = 0; p < PTS; p++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    u[p][c] = ub[(p * 3 + c) * NZ + j];
-                    ue[p][c] = u[p][c].x + u[p][c].y;
-                }
-            // sign table as in k_contract_tma; point p = slot * NP + vector, slot bits (sx, m)
-#define G2_TERM_L(C, K, IN, SGN)                                                 \
-    {                                                                            \
-        const R es_ = e[K].x + e[K].y;                                           \
-        _Pragma("unroll") for (int p = 0; p < PTS; p++)                          \
-        {                                                                        \
-            const int sl_ = p / NP;                                              \
-            const R sx = (sl_ & 2) ? R(-1) : R(1);                               \
-            const R m = (sl_ & 1) ? R(-1) : R(1);                                \
-            const R sg = (SGN);                                                  \
-            if constexpr (PK) {                                                  \
-                accp[C][p] = ffma2(sg < R(0) ? en[K] : e[K], u[p][IN], accp[C][p]); \
-                acc[C][p][NA - 1] = fma(sg * es_, ue[p][IN], acc[C][p][NA - 1]); \
-            } else if constexpr (M4) {                                           \
-                acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);       \
-                acc[C][p][0] = fma(-sg * e[K].y, u[p][IN].y, acc[C][p][0]);      \
-                acc[C][p][1] = fma(sg * e[K].x, u[p][IN].y, acc[C][p][1]);       \
-                acc[C][p][1] = fma(sg * e[K].y, u[p][IN].x, acc[C][p][1]);       \
-            } else {                                                             \
-                acc[C][p][0] = fma(sg * e[K].x, u[p][IN].x, acc[C][p][0]);       \
-                acc[C][p][1] = fma(sg * e[K].y, u[p][IN].y, acc[C][p][1]);       \
-                acc[C][p][NA - 1] = fma(sg * es_, ue[p][IN], acc[C][p][NA - 1]); \
-            }                                                                    \
-        }                                                                        \
-    }
-            G2_TERM_L(0, 0, 0, R(1))
-            G2_TERM_L(1, 1, 0, sx * m)
-            G2_TERM_L(2, 6, 0, -sx)
-            G2_TERM_L(0, 1, 1, sx * m)
-            G2_TERM_L(1, 2, 1, R(1))
-            G2_TERM_L(2, 7, 1, -m)
-            G2_TERM_L(0, 4, 2, sx)
-            G2_TERM_L(1, 5, 2, m)
-            G2_TERM_L(2, 3, 2, R(1))
-#undef G2_TERM_L
-        }
+        R v[Cfg::NR];
+        wl_unit_sums<R, NZ, SL, NP, M4, PK>(gb, ub, z, s, v);
         mbar_arrive(&empty[slot]);  // this lane's reads of the stage are done
 
-        R v[Cfg::NR];
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int p = 0; p < PTS; p++) {
-                if constexpr (PK) {
-                    const R t1 = accp[c][p].x, t2 = accp[c][p].y, t3 = acc[c][p][NA - 1];
-                    v[2 * (c * PTS + p)] = t1 - t2;
-                    v[2 * (c * PTS + p) + 1] = t3 - t1 - t2;
-                } else if constexpr (M4) {
-                    v[2 * (c * PTS + p)] = acc[c][p][0];
-                    v[2 * (c * PTS + p) + 1] = acc[c][p][1];
-                } else {
-                    const R t1 = acc[c][p][0], t2 = acc[c][p][1], t3 = acc[c][p][NA - 1];
-                    v[2 * (c * PTS + p)] = t1 - t2;
-                    v[2 * (c * PTS + p) + 1] = t3 - t1 - t2;
-                }
-            }
-        int f0 = 0;  // first flat output index this lane keeps
-        halve_slices<0, Cfg::NR, ZW, SL, Cfg::NR>(v, s, f0);
         const long long unit = first + it * stride;
         const int q = (int)(unit / Ny), r = (int)(unit - (long long)q * Ny);
-        C2 *dst = Uhat + unit * PTS * Cfg::Z3 + z;
-#pragma unroll
-        for (int i = 0; i < Cfg::HR; i += 2) {
-            const int k = (f0 + i) >> 1, c = k / PTS, p = k - c * PTS, sl = p / NP;
-            C2 o{v[i], v[i + 1]};
-            if ((q == 0 && (sl & 2)) || (r == 0 && (sl & 1))) o = C2{R(0), R(0)};
-            dst[(p * 3 + c) * NZ] = o;
-        }
+        wl_unit_store<R, NZ, SL, NP>(v, s, q, r, Uhat + unit * PTS * Cfg::Z3 + z);
     }
 }
 

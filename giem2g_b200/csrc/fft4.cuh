@@ -79,14 +79,17 @@ G2_D void reg_dft_dif(C (&a)[N], const C *tw, int Lstride)
 // LF1/LF2: item ordering (true: line index fastest across threads; false: n1 / k2 fastest).  Items are
 // split with shifts and masks of the power-of-two line block; lines >= nl (a partial last block) are
 // skipped.
+// The same transform run by a subset of the CTA's threads: thread tid of nthr, with sync() the barrier
+// of those threads (a named barrier when other warps of the CTA do other work).
 template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
-          class StoreF, class OffF>
-G2_D void fft4step(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF store, OffF off)
+          class StoreF, class OffF, class SyncF>
+G2_D void fft4step_part(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF store, OffF off, int tid, int nthr,
+                        SyncF sync)
 {
     constexpr int L = N1 * N2;
     const int nlb = 1 << lg_nl;
     const int n_items1 = (LF1 ? nlb : nl) * N1;
-    for (int it = threadIdx.x; it < n_items1; it += blockDim.x) {
+    for (int it = tid; it < n_items1; it += nthr) {
         int line, n1;
         if (LF1) { line = it & (nlb - 1); n1 = it >> lg_nl; }
         else { n1 = it % N1; line = it / N1; }
@@ -105,9 +108,9 @@ G2_D void fft4step(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF sto
             sm[off(line, n1, k2)] = v;
         }
     }
-    __syncthreads();
+    sync();
     const int n_items2 = (LF2 ? nlb : nl) * N2;
-    for (int it = threadIdx.x; it < n_items2; it += blockDim.x) {
+    for (int it = tid; it < n_items2; it += nthr) {
         int line, k2;
         if (LF2) { line = it & (nlb - 1); k2 = it >> lg_nl; }
         else { k2 = it % N2; line = it / N2; }
@@ -119,6 +122,15 @@ G2_D void fft4step(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF sto
 #pragma unroll
         for (int k1 = 0; k1 < (CROP_OUT ? N1 / 2 : N1); k1++) store(line, k2 + N2 * k1, a[brev_c(k1, Log2<N1>::v)]);
     }
+}
+
+// The whole CTA transforms its line block.
+template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
+          class StoreF, class OffF>
+G2_D void fft4step(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF store, OffF off)
+{
+    fft4step_part<C, N1, N2, INV, PAD_IN, CROP_OUT, LF1, LF2>(sm, nl, lg_nl, tw, load, store, off, (int)threadIdx.x,
+                                                              (int)blockDim.x, [] { __syncthreads(); });
 }
 
 // factorisation L = N1 * N2 used by the transform kernels

@@ -55,6 +55,9 @@ struct IeOp {
     int precision_mode = 0;            // 0 plain FP64, 1 mixed (c64 inner)
     bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
     int contract_variant[3] = {0, 0, 0};  // tile-shape variant: FP64, complex64, paired complex64
+    // fused y-transforms + contraction (ypipe.cu) per form: its variant, or -1 for the separate passes
+    // (k_fy, contraction, k_by); used where ie_ypipe_supported holds (GIEM2G_NO_YPIPE=1 starts at -1)
+    int ypipe_mode[3] = {0, 0, 0};
     int fft_lines[2] = {32, 32};          // lines per CTA of the FFT passes, complex128 / complex64 (autotuned)
     long long config_gen = 0;             // bumped on every launch-shape change; captured graphs compare it
     // outer right-preconditioner hook (learned preconditioner): 0 off, 1 warm-starts the inner GMRES,
@@ -109,7 +112,15 @@ int ie_gemm_bf16_tn(const void *A, const void *B, float *C, int M, int N, int K,
                     int accumulate, int *err, cudaStream_t st);
 int ie_alloc_scratch(IeOp *op);
 int ie_make_twiddles(IeOp *op);
-int ie_kernel_launch_count_apply();
+// kernels one apply launches in a form (0 FP64, 1 complex64, 2 paired complex64)
+int ie_kernel_launch_count_apply(const IeOp *op, int form);
+
+// ypipe.cu: forward y-FFT, contraction and inverse y-FFT in one persistent kernel (U1 in, U1 out, the
+// spectrum Uh as scratch, `state` = ie_ypipe_state_bytes of counters zeroed by the launcher)
+bool ie_ypipe_supported(int Nx, int Ny, int Nz);
+int ie_ypipe_variants(int form);
+size_t ie_ypipe_state_bytes(int Nx);
+int ie_ypipe(IeOp *op, int form, const void *G, void *U1, void *Uh, int *state, cudaStream_t st, const int *gate);
 
 // learned_net.cu: the U-Net outer preconditioner (kind 0 off, 1 warm start, 2 replace)
 int ie_set_learned_preconditioner(IeOp *op, int kind, const char *weights_path);
