@@ -501,6 +501,24 @@ def run_b200(args, rank, world, local_rank):
 
     rcv = time_receivers() if rank == 0 else None
 
+    # the batched multi-frequency sweep on this grid: 8 frequencies (1e-3 .. 1e2 Hz) x 2 polarisations = 16
+    # lockstep instances in mixed precision, against the same 16 solved one after the other in plain FP64
+    sweep = None
+    if rank == 0 and not args.no_sweep:
+        try:
+            from giem2g_b200.sweep import run_sweep
+            res = run_sweep(m, sig, list(np.logspace(-3, 2, 8)), tol=TOL, compare=True, tuned=tuned)
+            sweep = {"instances": len(res["batched"]["iterations"]), "freqs_hz": res["freqs"],
+                     "batched_mixed_ms": res["batched"]["device_ms"],
+                     "sequential_mixed_ms": res["sequential_mixed"]["device_ms"],
+                     "sequential_fp64_ms": res["sequential_fp64"]["device_ms"],
+                     "speedup_vs_sequential_fp64": res["speedup_batched_vs_sequential_fp64"],
+                     "outer_iterations": res["batched"]["iterations"], "stat": res["batched"]["stat"],
+                     "max_field_error_vs_fp64": max(res["field_error_vs_fp64"]),
+                     "setup_s_per_frequency": res["setup_s_per_frequency"]}
+        except Exception as exc:  # reported, never the headline
+            sweep = {"error": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -562,6 +580,7 @@ def run_b200(args, rank, world, local_rank):
                       "field_error_vs_fp64_tol1e-8": [err_y, err_x]},
             "learned_preconditioner": learned,
             "receiver_fields": rcv,
+            "sweep_8freq_x2pol": sweep,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }
@@ -672,6 +691,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the 16-instance multi-frequency sweep")
     ap.add_argument("--variants", default=None,
                     help="pin the tile shapes instead of autotuning: v64,v32,vpair[,fft_lines[,fft_lines64]] "
                          "(for profilers)")

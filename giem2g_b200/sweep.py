@@ -40,7 +40,9 @@ def sweep_config(name: str):
 
 
 def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner=10, max_restart=100,
-              compare=False, fp64_tol=1e-8):
+              compare=False, fp64_tol=1e-8, tuned=None):
+    """`tuned`: tile shapes to pin on every operator (an autotune_contraction result of the same grid);
+    without it the shapes are timed on the first operator."""
     import torch
     import giem2g_b200 as g2
     from .sources import plane_wave_integral
@@ -60,8 +62,10 @@ def run_sweep(m, sig, freqs, pols=(1, 0), tol=1e-6, precision=1, outer=30, inner
     out["setup_s_per_frequency"] = setup_s
     # tile shapes: time the variants on the first operator; the others have the same grid
     from .autotune import autotune_contraction
-    tuned = autotune_contraction(ops[0][1])
-    for _, op in ops[1:]:
+    pinned = tuned is not None
+    if not pinned:
+        tuned = autotune_contraction(ops[0][1])
+    for _, op in (ops if pinned else ops[1:]):
         for prec in (0, 1, 2):
             if str(prec) in tuned and op.contract_variants(prec) > 1:
                 op.set_contract_variant(prec, tuned[str(prec)]["variant"])

@@ -137,3 +137,61 @@ def test_batched_solve_zero_rhs_instance(g2lib):
     b.delete()
     for op in ops:
         op.delete()
+
+
+def test_eight_instance_sweep_batch(g2lib, orc):
+    """Four frequencies x two polarisations (8 lockstep instances, the multi-frequency sweep's form) on a
+    32x32x32 model whose applies take the fused y-pass: in FP64 every instance reproduces its own single solve
+    (iterations, status, solution within 1e-12); in mixed precision every instance converges to outer
+    relative residual 1e-6 and lies within 1e-5 of its FP64 solution (tol 1e-10).  One FP64 solution is put
+    back through the oracle's apply of the same tensor: its recomputed relative residual stays within 1.5x
+    the tolerance."""
+    import torch
+    from giem2g_b200.synthetic import config_grf
+    m0, sig = config_grf(32, 32, 32, seed=9)
+    freqs = [0.01, 0.3, 3.0, 30.0]
+    ops, inst = [], []
+    for f in freqs:
+        m = m0.with_freq(f)
+        op = g2lib.IEOperator.from_model(m)
+        op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+        op.calc_fft_of_ie_kernel()
+        op.set_anomaly_sigma(sig, m.freq)
+        ops.append((m, op))
+        for pol in (1, 0):
+            inst.append((m, op, plane_wave_integral(m, pol)))
+    assert len(inst) == 8
+    d_e = [torch.from_numpy(np.ascontiguousarray(e).ravel()).to("cuda") for _, _, e in inst]
+    ref64, single64 = [], []
+    for (_, op, _), x in zip(inst, d_e):
+        y = torch.empty_like(x)
+        op.solve_device(x.data_ptr(), y.data_ptr(), None, tol=1e-10, precision=0)
+        ref64.append(y)
+        y8 = torch.empty_like(x)
+        single64.append((op.solve_device(x.data_ptr(), y8.data_ptr(), None, tol=1e-8, precision=0), y8))
+    for precision, tol in ((0, 1e-8), (1, 1e-6)):
+        d_s = [torch.empty_like(x) for x in d_e]
+        b = g2lib.Batch([op for _, op, _ in inst], precision=precision)
+        infos = b.solve_device([x.data_ptr() for x in d_e], [y.data_ptr() for y in d_s], tol=tol)
+        torch.cuda.synchronize()
+        for i, info in enumerate(infos):
+            assert info.stat == 1 and info.be < tol, (precision, i, info)
+            if precision == 0:
+                s_info, s_y = single64[i]
+                assert info.iterations == s_info.iterations
+                assert rel(d_s[i].cpu().numpy(), s_y.cpu().numpy()) < 1e-12
+            else:
+                assert rel(d_s[i].cpu().numpy(), ref64[i].cpu().numpy()) < 1e-5, i
+        b.delete()
+    # one FP64 solution through the oracle's apply (SolveEquation's system A chi = sqrt(Re sigma_b) E0)
+    m, op, E0 = inst[2]
+    sh, ah = op.get_ie_kernel_spectral()
+    csiga = csiga_from_sigma(sig, m.freq)
+    csigb, sqsigb = orc.background_cells(m)
+    E = single64[2][1].cpu().numpy().reshape(E0.shape)
+    a = 2.0 * sqsigb[:, None, None] / (csiga + np.conj(csigb)[:, None, None])
+    rhs = sqsigb[None, :, None, None] * E0
+    r = orc.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, E / a[None]) - rhs
+    assert np.linalg.norm(r) / np.linalg.norm(rhs) < 1.5e-8
+    for _, op in ops:
+        op.delete()
