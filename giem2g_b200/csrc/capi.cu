@@ -143,8 +143,6 @@ void giem2g_prepare_ie_kernel(GIEM2G_ANOMALY_TYPE anomaly, GIEM2G_DATA_TYPE data
     {
         const char *gen = std::getenv("GIEM2G_GENERIC_CONTRACT");
         op->use_fast_contract = !(gen && gen[0] == '1');
-        const char *noy = std::getenv("GIEM2G_NO_YPIPE");
-        if (noy && noy[0] == '1') op->ypipe_mode[0] = op->ypipe_mode[1] = op->ypipe_mode[2] = -1;
     }
     int rc = ie_make_twiddles(op);
     if (!rc) rc = ie_alloc_scratch(op);

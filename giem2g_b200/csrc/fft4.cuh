@@ -124,6 +124,54 @@ G2_D void fft4step_part(C *sm, int nl, int lg_nl, const C *tw, LoadF load, Store
     }
 }
 
+// fft4step_part for a fixed number of step-1 items per thread (IPT * nthr >= the items): every thread issues
+// the loads of all its items before the first register DFT, so the transform waits for one load round trip
+// instead of one per item (for a few warps that transform tasks one after another).
+template <typename C, int N1, int N2, int IPT, bool INV, bool PAD_IN, bool CROP_OUT, class LoadF, class StoreF,
+          class OffF, class SyncF>
+G2_D void fft4step_part_ilp(C *sm, int nl, int lg_nl, const C *tw, LoadF load, StoreF store, OffF off, int tid,
+                            int nthr, SyncF sync)
+{
+    constexpr int L = N1 * N2;
+    constexpr int NLD = PAD_IN ? N2 / 2 : N2;
+    const int nlb = 1 << lg_nl;
+    const int n_items1 = nlb * N1;  // line index fastest
+    C a[IPT][N2];
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        const int it = tid + r * nthr;
+        const int line = it & (nlb - 1), n1 = it >> lg_nl;
+        const bool ok = it < n_items1 && line < nl;
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) a[r][n2] = (ok && n2 < NLD) ? load(line, n1 + N1 * n2) : czero<C>();
+    }
+#pragma unroll
+    for (int r = 0; r < IPT; r++) {
+        const int it = tid + r * nthr;
+        const int line = it & (nlb - 1), n1 = it >> lg_nl;
+        if (it >= n_items1 || line >= nl) continue;
+        reg_dft_dif<C, N2, INV, PAD_IN>(a[r], tw, L / N2);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            C v = a[r][brev_c(k2, Log2<N2>::v)];
+            if (k2 != 0 && n1 != 0) v = cmul(v, twid<C, INV>(tw, n1 * k2));
+            sm[off(line, n1, k2)] = v;
+        }
+    }
+    sync();
+    const int n_items2 = nlb * N2;
+    for (int it = tid; it < n_items2; it += nthr) {
+        const int line = it & (nlb - 1), k2 = it >> lg_nl;
+        if (line >= nl) continue;
+        C b[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) b[n1] = sm[off(line, n1, k2)];
+        reg_dft_dif<C, N1, INV, false>(b, tw, L / N1);
+#pragma unroll
+        for (int k1 = 0; k1 < (CROP_OUT ? N1 / 2 : N1); k1++) store(line, k2 + N2 * k1, b[brev_c(k1, Log2<N1>::v)]);
+    }
+}
+
 // The whole CTA transforms its line block.
 template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
           class StoreF, class OffF>

@@ -56,8 +56,9 @@ struct IeOp {
     bool use_fast_contract = true;     // GIEM2G_GENERIC_CONTRACT=1 selects the generic contraction kernel
     int contract_variant[3] = {0, 0, 0};  // tile-shape variant: FP64, complex64, paired complex64
     // fused y-transforms + contraction (ypipe.cu) per form: its variant, or -1 for the separate passes
-    // (k_fy, contraction, k_by); used where ie_ypipe_supported holds (GIEM2G_NO_YPIPE=1 starts at -1)
-    int ypipe_mode[3] = {0, 0, 0};
+    // (k_fy, contraction, k_by).  The separate passes are the default (faster at 128x128x32 on a B200);
+    // the fused pass is a tile-shape variant the autotuner may pick where ie_ypipe_supported holds.
+    int ypipe_mode[3] = {-1, -1, -1};
     int fft_lines[2] = {32, 32};          // lines per CTA of the FFT passes, complex128 / complex64 (autotuned)
     long long config_gen = 0;             // bumped on every launch-shape change; captured graphs compare it
     // outer right-preconditioner hook (learned preconditioner): 0 off, 1 warm-starts the inner GMRES,

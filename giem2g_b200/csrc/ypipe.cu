@@ -1,5 +1,11 @@
-// The y-transforms fused with the Green's-tensor contraction: one persistent kernel per apply replaces
-// k_fy -> contraction -> k_by (apply.cu), so the 2-D spectrum never makes a round trip through HBM.
+// The y-transforms fused with the Green's-tensor contraction: one persistent kernel in place of
+// k_fy -> contraction -> k_by (apply.cu), so the 2-D spectrum never makes a round trip through HBM.  It is
+// a tile-shape variant (giem2g_set_contract_variant, the last two of each form at Nz = 32), not the default:
+// measured on a B200 at 128x128x32 the separate passes are faster (FP64 apply 0.33 against 0.47 ms).  Three
+// FFT warps per SM need about 0.1 ms for the y-transforms of one apply on their own, and the FP64 stage
+// ring has room for two stages beside the transform lines, so the pass costs about what the spectrum's round
+// trip saves (both roles timed apart in a probe: FP64 contraction role 0.26-0.29 ms, FFT role 0.16 ms;
+// complex64 0.12 and 0.10 ms; the separate k_fy + contraction + k_by take 0.27 and 0.17 ms).
 //
 // Restates the middle of MULT_IE_OP (apply_ie_operator_module.F90:189-263): the forward y-FFT with its +-ky
 // repack (Distributed_FFT.F90:437-505), VERTICAL_MULT_GENERAL at every (kx-pair, ky-pair) unit
@@ -43,6 +49,7 @@
 namespace {
 
 constexpr int kQB = 4;            // kx pairs per batch
+constexpr int kChunk = 2;         // units per grab of a producer
 constexpr int kStateHead = 4;     // next_unit, next_task, two spare
 constexpr uint64_t kWaitNs = 2000000000ull;
 
@@ -65,6 +72,7 @@ struct CfgY {
     static constexpr int N1 = Fact<L>::N1, N2 = Fact<L>::N2;
     static constexpr int LG_NL = Log2<NL>::v;
     static constexpr int NBLK = (ZL + NL - 1) / NL;        // line blocks per column
+    static constexpr int IPT = (NL * N1 + NF - 1) / NF;    // step-1 items per FFT thread
     static constexpr int FFT_ELEMS = L + NL * (L + 1);     // twiddles + lines
     static constexpr int OFF_FFT = NSTAGE * STAGE_BYTES;
     static constexpr int OFF_BAR = OFF_FFT + FFT_ELEMS * ES;
@@ -161,11 +169,14 @@ __global__ void __launch_bounds__(CfgY<R, L, NZ, NP, SL, NG, NSTAGE, PK, NFW, NL
         const int ftid = tid - (Cfg::NC + 32);
         auto fsync = [] { named_bar_sync(1, Cfg::NF); };
         const int n_tasks = 2 * nb * fpb;
+        // the next task is grabbed while the current one runs (the atomic's round trip is hidden)
+        if (ftid == 0) *s_task = atomicAdd(next_task, 1);
+        fsync();
         while (true) {
-            if (ftid == 0) *s_task = atomicAdd(next_task, 1);
-            fsync();
             const int t = *s_task;
             fsync();
+            int t_next = 0;
+            if (ftid == 0 && t < n_tasks) t_next = atomicAdd(next_task, 1);
             if (t >= n_tasks) break;
             // segments: F(0), F(1), I(0), F(2), I(1), ..., F(nb-1), I(nb-2), I(nb-1)
             const int seg = t / fpb, within = t - seg * fpb;
@@ -197,7 +208,7 @@ __global__ void __launch_bounds__(CfgY<R, L, NZ, NP, SL, NG, NSTAGE, PK, NFW, NL
                         else { r = 2 * Ny - ky; sy = 1; }
                         spec[(r * 4 + sy) * ZL + t2] = v;
                     };
-                    fft4step_part<C2, Cfg::N1, Cfg::N2, false, true, false, true, true>(
+                    fft4step_part_ilp<C2, Cfg::N1, Cfg::N2, Cfg::IPT, false, true, false>(
                         fsm, nl, Cfg::LG_NL, ftw, load, store, off, ftid, Cfg::NF, fsync);
                 } else {
                     auto load = [&](int t2, int ky) -> C2 {
@@ -208,15 +219,17 @@ __global__ void __launch_bounds__(CfgY<R, L, NZ, NP, SL, NG, NSTAGE, PK, NFW, NL
                         return ld_l2(&spec[(r * 4 + sy) * ZL + t2]);
                     };
                     auto store = [&](int t2, int yy, C2 v) { col[yy * ZL + t2] = v; };
-                    fft4step_part<C2, Cfg::N1, Cfg::N2, true, false, true, true, true>(
+                    fft4step_part_ilp<C2, Cfg::N1, Cfg::N2, Cfg::IPT, true, false, true>(
                         fsm, nl, Cfg::LG_NL, ftw, load, store, off, ftid, Cfg::NF, fsync);
                 }
             }
-            if (fwd) {
-                __threadfence();
-                fsync();
-                if (ftid == 0) atomicAdd(&f_done[b], 1);
+            if (fwd) __threadfence();
+            fsync();  // every thread is done with the task (and its shared lines) before the next one
+            if (ftid == 0) {
+                if (fwd) atomicAdd(&f_done[b], 1);
+                *s_task = t_next;
             }
+            fsync();
         }
         return;
     }
@@ -228,12 +241,20 @@ __global__ void __launch_bounds__(CfgY<R, L, NZ, NP, SL, NG, NSTAGE, PK, NFW, NL
         const uint64_t pol_u = l2_policy_evict_normal();
         int it = 0, ready_b = -1;
         bool ok = true;
+        // units are grabbed kChunk at a time, and the next chunk is grabbed while this one is issued, so the
+        // atomic's round trip stays out of the stage-refill path
+        int u = atomicAdd(next_unit, kChunk), u_end = u + kChunk;
+        int u_next = atomicAdd(next_unit, kChunk);
         while (true) {
+            if (u >= u_end) {
+                u = u_next;
+                u_end = u + kChunk;
+                if (u < total_units) u_next = atomicAdd(next_unit, kChunk);
+            }
+            if (u >= total_units) break;
             const int slot = it % NSTAGE;
             const uint32_t round = (uint32_t)(it / NSTAGE);
             if (round > 0 && !mbar_wait_bounded(&empty[slot], (round - 1) & 1, err, 41)) { ok = false; break; }
-            const int u = atomicAdd(next_unit, 1);
-            if (u >= total_units) break;
             unsigned char *st = stages + slot * Cfg::STAGE_BYTES;
             unit_of[slot] = u;
             mbar_arrive_expect_tx(&full[slot], Cfg::STAGE_BYTES);
@@ -247,6 +268,7 @@ __global__ void __launch_bounds__(CfgY<R, L, NZ, NP, SL, NG, NSTAGE, PK, NFW, NL
             }
             bulk_g2s(st + Cfg::TBYTES, Uh + (size_t)u * 4 * ZL, Cfg::UBYTES, &full[slot], pol_u);
             it++;
+            u++;
         }
         if (ok) {
             // one end-of-work ticket per consumer group
@@ -331,16 +353,17 @@ int launch_y(const YArgs &a, size_t state_bytes, cudaStream_t st)
 template <int L>
 int dispatch_nz32(int prec, int variant, const YArgs &a, size_t sb, cudaStream_t st)
 {
+    constexpr int NLW = L >= 512 ? 8 : 16;  // lines per transform task (the 2Ny = 512 tile is twice as long)
     if (prec == 0) {
-        if (variant == 1) return launch_y<double, L, 32, 1, 4, 2, 2, false, 3, 4>(a, sb, st);
-        return launch_y<double, L, 32, 1, 4, 2, 2, false, 3, 8>(a, sb, st);
+        if (variant == 1) return launch_y<double, L, 32, 1, 4, 2, 2, false, 3, 8>(a, sb, st);
+        return launch_y<double, L, 32, 1, 4, 2, 2, false, 3, NLW>(a, sb, st);
     }
     if (prec == 1) {
-        if (variant == 1) return launch_y<float, L, 32, 1, 2, 4, 5, true, 3, 8>(a, sb, st);
-        return launch_y<float, L, 32, 1, 2, 6, 5, true, 3, 8>(a, sb, st);
+        if (variant == 1) return launch_y<float, L, 32, 1, 2, 4, 5, true, 3, NLW>(a, sb, st);
+        return launch_y<float, L, 32, 1, 2, 6, 5, true, 3, NLW>(a, sb, st);
     }
-    if (variant == 1) return launch_y<float, L, 32, 2, 2, 4, (L >= 512 ? 4 : 5), true, 3, (L >= 512 ? 4 : 8)>(a, sb, st);
-    return launch_y<float, L, 32, 2, 2, 4, 4, true, 3, 8>(a, sb, st);
+    if (variant == 1) return launch_y<float, L, 32, 2, 2, 4, 4, true, 3, 8>(a, sb, st);
+    return launch_y<float, L, 32, 2, 2, 4, 4, true, 3, NLW>(a, sb, st);
 }
 
 }  // namespace

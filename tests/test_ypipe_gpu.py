@@ -73,6 +73,7 @@ def test_fused_apply_launches_three_kernels(g2lib):
     op, *_ = _op(g2lib, m)
     x = torch.from_numpy(random_vec(m, 5).ravel()).to("cuda")
     y = torch.empty_like(x)
+    op.set_contract_variant(0, op.contract_variants(0) - 2)  # the fused pass, variant 0
     n0 = g2lib.kernel_launch_count()
     op.apply_device(x.data_ptr(), y.data_ptr(), 0)
     assert g2lib.kernel_launch_count() - n0 == 3 and op.last_kernel_launches() == 3
@@ -88,6 +89,7 @@ def test_fused_apply_repeats_exactly(g2lib):
     import torch
     m = tiny_model(64, 64, 32)
     op, *_ = _op(g2lib, m)
+    op.set_contract_variant(1, op.contract_variants(1) - 2)  # the fused pass, variant 0
     x = torch.from_numpy(random_vec(m, 6).ravel()).to("cuda", torch.complex64)
     y0, y = torch.empty_like(x), torch.empty_like(x)
     op.apply_device(x.data_ptr(), y0.data_ptr(), 1)
