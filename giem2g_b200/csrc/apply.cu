@@ -177,21 +177,23 @@ __global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, c
     auto load = [&](int t, int kx) -> C {
         return kx == Nx ? czero<C>() : U1[(kx * Ny + y) * ZL + zc0 + t];
     };
-    auto store = [&](int t, int x, C w) {
+    // a*x of each output, read before the inverse transform of its line (see fft4step_pre)
+    auto pre = [&](int t, int x) -> C {
         const int zc = zc0 + t, v = zc >= Z3 ? 1 : 0, lzc = zc - v * Z3, z = lzc % Nz;
-        const int cell = z * plane + row + x;
-        const int idx = lzc * plane + row + x;
         const C *in = v ? vs.in[1] : vs.in[0];
+        return cmul(in[lzc * plane + row + x], asig[z * plane + row + x]);
+    };
+    auto store = [&](int t, int x, C w, C d1) {
+        const int zc = zc0 + t, v = zc >= Z3 ? 1 : 0, lzc = zc - v * Z3, z = lzc % Nz;
         C *out = v ? vs.out[1] : vs.out[0];
-        const C d1 = cmul(in[idx], asig[cell]);
         const R sq = post[z], inv = post[Nz + z];
         C o;
         o.x = (d1.x - w.x * inv) * sq;
         o.y = (d1.y - w.y * inv) * sq;
-        out[idx] = o;
+        out[lzc * plane + row + x] = o;
     };
     auto off = [&](int t, int n1, int k2) { return t * (L + 1) + k2 + N2 * n1; };
-    fft4step<C, N1, N2, true, false, true, true, false>(sm, nl, ilog2(NL), tw, load, store, off);
+    fft4step_pre<C, N1, N2, true, false, true, true, false>(sm, nl, ilog2(NL), tw, load, pre, store, off);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -172,6 +172,57 @@ G2_D void fft4step_part_ilp(C *sm, int nl, int lg_nl, const C *tw, LoadF load, S
     }
 }
 
+// fft4step for a store that needs other data at each output (an epilogue): pre(line, idx) returns it and is
+// called for all of an item's outputs before the item's shared-memory loads and register DFT, so those global
+// loads are in flight together (a store functor that loads would otherwise wait once per output: the
+// compiler may not move a load above an earlier store to possibly aliasing memory); store(line, idx, v, p).
+// Each output's data is read before that thread stores any output, so in-place vectors stay correct.
+template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
+          class PreF, class StoreF, class OffF>
+G2_D void fft4step_pre(C *sm, int nl, int lg_nl, const C *tw, LoadF load, PreF pre, StoreF store, OffF off)
+{
+    constexpr int L = N1 * N2;
+    constexpr int NOUT = CROP_OUT ? N1 / 2 : N1;
+    const int nlb = 1 << lg_nl;
+    const int n_items1 = (LF1 ? nlb : nl) * N1;
+    for (int it = threadIdx.x; it < n_items1; it += blockDim.x) {
+        int line, n1;
+        if (LF1) { line = it & (nlb - 1); n1 = it >> lg_nl; }
+        else { n1 = it % N1; line = it / N1; }
+        if (LF1 && line >= nl) continue;
+        C a[N2];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) {
+            if (PAD_IN && n2 >= N2 / 2) a[n2] = czero<C>();
+            else a[n2] = load(line, n1 + N1 * n2);
+        }
+        reg_dft_dif<C, N2, INV, PAD_IN>(a, tw, L / N2);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            C v = a[brev_c(k2, Log2<N2>::v)];
+            if (k2 != 0 && n1 != 0) v = cmul(v, twid<C, INV>(tw, n1 * k2));
+            sm[off(line, n1, k2)] = v;
+        }
+    }
+    __syncthreads();
+    const int n_items2 = (LF2 ? nlb : nl) * N2;
+    for (int it = threadIdx.x; it < n_items2; it += blockDim.x) {
+        int line, k2;
+        if (LF2) { line = it & (nlb - 1); k2 = it >> lg_nl; }
+        else { k2 = it % N2; line = it / N2; }
+        if (LF2 && line >= nl) continue;
+        decltype(pre(0, 0)) p[NOUT];
+#pragma unroll
+        for (int k1 = 0; k1 < NOUT; k1++) p[k1] = pre(line, k2 + N2 * k1);
+        C a[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; n1++) a[n1] = sm[off(line, n1, k2)];
+        reg_dft_dif<C, N1, INV, false>(a, tw, L / N1);
+#pragma unroll
+        for (int k1 = 0; k1 < NOUT; k1++) store(line, k2 + N2 * k1, a[brev_c(k1, Log2<N1>::v)], p[k1]);
+    }
+}
+
 // The whole CTA transforms its line block.
 template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
           class StoreF, class OffF>

@@ -192,7 +192,18 @@ G2_D void reduce_partials(const double2 *part, int nb, int K, double2 *h, double
     for (int k = warp; k <= K; k += nw) {
         const int col = (k == K) ? KMAX : k;
         double sx = 0.0, sy = 0.0;
-        for (int b = lane; b < nb; b += 32) {
+        // four independent loads per lane and round: the partials come from L2, and a chain of dependent
+        // loads (one per 32 blocks) made this tail cost several microseconds per reduction
+        int b = lane;
+        for (; b + 96 < nb; b += 128) {
+            const double2 v0 = __ldcg(part + (size_t)b * (KMAX + 1) + col);
+            const double2 v1 = __ldcg(part + (size_t)(b + 32) * (KMAX + 1) + col);
+            const double2 v2 = __ldcg(part + (size_t)(b + 64) * (KMAX + 1) + col);
+            const double2 v3 = __ldcg(part + (size_t)(b + 96) * (KMAX + 1) + col);
+            sx += (v0.x + v1.x) + (v2.x + v3.x);
+            sy += (v0.y + v1.y) + (v2.y + v3.y);
+        }
+        for (; b < nb; b += 32) {
             const double2 v = __ldcg(part + (size_t)b * (KMAX + 1) + col);
             sx += v.x;
             sy += v.y;
@@ -211,15 +222,42 @@ G2_D void reduce_partials(const double2 *part, int nb, int K, double2 *h, double
 }
 
 // first CGS pass of Arnoldi step j = K-1: h = V^H w, then H(0..j, j) = h, hpass = h
+// elements per thread and round of the basis sweeps: all (K + 1) * U loads of a round are issued before the
+// first product, so a round costs one memory round trip; the values held stay within 256 bytes per thread
+// (32 complex64 or 16 complex128).  0: the basis is too wide to hold, the sweep loads one element at a time.
+template <int K, typename C> struct SweepU {
+    static constexpr int B = (K + 1) * (int)sizeof(C);
+    static constexpr int v = B * 4 <= 256 ? 4 : (B * 2 <= 256 ? 2 : (B <= 256 ? 1 : 0));
+};
+
 template <typename C, int K>
 G2_D void dots_first_body(const C *__restrict__ V, size_t ld, const C *__restrict__ w, size_t N, double2 *part,
                           Level &L)
 {
     using R = typename RealOf<C>::T;
+    constexpr int U = SweepU<K, C>::v > 0 ? SweepU<K, C>::v : 1;
     R ax[K + 1], ay[K + 1];
 #pragma unroll
     for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+    const size_t S = (size_t)gridDim.x * kVT;
+    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
+    for (; SweepU<K, C>::v > 0 && i + (U - 1) * S < N; i += U * S) {
+        C wv[U], v[K > 0 ? K : 1][U];
+#pragma unroll
+        for (int u = 0; u < U; u++) wv[u] = w[i + u * S];
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int u = 0; u < U; u++) v[k][u] = V[(size_t)k * ld + i + u * S];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                ax[k] += v[k][u].x * wv[u].x + v[k][u].y * wv[u].y;
+                ay[k] += v[k][u].x * wv[u].y - v[k][u].y * wv[u].x;
+            }
+    }
+    for (; i < N; i += S) {
         const C wv = w[i];
 #pragma unroll
         for (int k = 0; k < K; k++) {
@@ -276,7 +314,36 @@ G2_D void cgs_pass_body(const C *__restrict__ V, size_t ld, C *__restrict__ w, s
     R ax[K + 1], ay[K + 1];
 #pragma unroll
     for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+    constexpr int U = SweepU<K, C>::v > 0 ? SweepU<K, C>::v : 1;
+    const size_t S = (size_t)gridDim.x * kVT;
+    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
+    // U elements per round, every load of the round first; the basis values stay in registers for the dots
+    for (; SweepU<K, C>::v > 0 && i + (U - 1) * S < N; i += U * S) {
+        C wv[U], v[K > 0 ? K : 1][U];
+#pragma unroll
+        for (int u = 0; u < U; u++) wv[u] = w[i + u * S];
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int u = 0; u < U; u++) v[k][u] = V[(size_t)k * ld + i + u * S];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const R hx = (R)hsh[k].x, hy = (R)hsh[k].y;
+                wv[u].x -= v[k][u].x * hx - v[k][u].y * hy;
+                wv[u].y -= v[k][u].x * hy + v[k][u].y * hx;
+            }
+            w[i + u * S] = wv[u];
+            ax[K] += wv[u].x * wv[u].x + wv[u].y * wv[u].y;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                ax[k] += v[k][u].x * wv[u].x + v[k][u].y * wv[u].y;
+                ay[k] += v[k][u].x * wv[u].y - v[k][u].y * wv[u].x;
+            }
+        }
+    }
+    for (; i < N; i += S) {
         C wv = w[i];
 #pragma unroll
         for (int k = 0; k < K; k++) {
