@@ -24,6 +24,7 @@ set-up.  The line reports the full solves' own rate beside it.
 Profiler workloads (no JSON contract; one line of timings):
   --apply-only      a few IE applies at a given grid (kernels k_fx, k_fy, contraction, k_by, k_bx)
   --receivers-only  the receiver-field tensor build and a few recalculations
+  --step-breakdown  warm per-kernel device times of one batched step
 """
 from __future__ import annotations
 
@@ -196,8 +197,11 @@ def run_reference(args, rank, world):
     for _ in range(3):
         oracle.apply(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, v, nthreads=ncores)
     t_apply = (time.perf_counter() - t0) / 3
-    # full solves of both polarisations: outer-iteration counts and the true solve times
+    # full solves of both polarisations: outer-iteration counts and the true solve times (after one untimed
+    # full solve: the first solve of a process also pays its thread start-up and first touches of the work space)
     pols = [("EY", e_y), ("EX", e_x)]
+    oracle.solve(m.Nx, m.Ny, m.Nz, sh, ah, csiga, csigb, sqsigb, m.dz, e_y, None, OUTER, INNER, MAXRESTART, TOL,
+                 nthreads=ncores)
     n_outer, t_full, applies = [], [], []
     for _, rhs in pols:
         t0 = time.perf_counter()
@@ -684,6 +688,62 @@ def run_receivers_only(args):
     return 0
 
 
+def run_step_breakdown(args):
+    """Warm per-kernel device times of one batched benchmark step (the CUPTI activity trace torch.profiler
+    records; every kernel of the process, this library's included), with the step's CUDA-event time taken
+    without the profiler and the idle gaps between kernels.  Prints one JSON line."""
+    import collections
+    import torch
+    import giem2g_b200 as g2
+    from giem2g_b200.autotune import autotune_contraction, pin_contraction
+    from torch.profiler import ProfilerActivity, profile
+    g2.set_logger(lambda msg: None)
+    m, sig, e_y, e_x = build_problem()
+    op = g2.IEOperator.from_model(m)
+    op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+    op.calc_fft_of_ie_kernel()
+    op.set_anomaly_sigma(sig, m.freq)
+    tuned = pin_contraction(op, args.variants) if args.variants else autotune_contraction(op)
+    dev = torch.device("cuda")
+    d_in = [torch.from_numpy(np.ascontiguousarray(e).ravel()).to(dev) for e in (e_y, e_x)]
+    d_out = [torch.empty_like(x) for x in d_in]
+    batch = g2.Batch([op, op], outer_buf=OUTER, inner_buf=INNER, precision=1, max_restart=MAXRESTART)
+
+    def step():
+        return batch.solve_device([x.data_ptr() for x in d_in], [y.data_ptr() for y in d_out], tol=TOL)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(op.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1)
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step()
+        torch.cuda.synchronize()
+    tot, cnt, iv = collections.Counter(), collections.Counter(), []
+    for e in prof.events():
+        if e.device_type != torch.autograd.DeviceType.CUDA:
+            continue
+        name = e.name.split("<")[0].split("(")[0].replace("void ", "").replace("(anonymous namespace)::", "").strip()
+        tot[name] += e.device_time_total
+        cnt[name] += 1
+        iv.append((e.time_range.start, e.time_range.end))
+    iv.sort()
+    gaps = [b[0] - a[1] for a, b in zip(iv, iv[1:]) if b[0] > a[1]]
+    print(json.dumps({"mode": "step-breakdown", "step_ms": step_ms, "kernels": sum(cnt.values()),
+                      "busy_ms": sum(tot.values()) / 1e3, "idle_gap_ms": sum(gaps) / 1e3,
+                      "per_kernel_ms": {k: [round(v / 1e3, 4), cnt[k]] for k, v in tot.most_common()},
+                      "contract_variants": {k: v.get("variant", v.get("lines")) for k, v in tuned.items()}}))
+    batch.delete()
+    op.delete()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -707,9 +767,13 @@ def main():
     prof.add_argument("--nv", type=int, default=1, choices=[1, 2], help="vectors per apply (2: paired complex64)")
     prof.add_argument("--fft-lines", type=int, default=None, choices=[4, 8, 16, 32])
     prof.add_argument("--nr", type=int, default=1, help="receiver depths")
+    prof.add_argument("--step-breakdown", action="store_true",
+                      help="warm per-kernel device times of one batched step (CUPTI trace)")
     args = ap.parse_args()
     if args.apply_only:
         return run_apply_only(args)
+    if args.step_breakdown:
+        return run_step_breakdown(args)
     if args.receivers_only:
         if args.warmup == ap.get_default("warmup"):
             args.warmup = 1
