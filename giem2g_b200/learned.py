@@ -13,10 +13,13 @@ im2col (bf16), the tcgen05 BF16 GEMM with FP32 accumulation (giem2g_gemm_bf16_tn
 col2im.  Weights and activations enter the GEMMs in BF16; ReLU, nearest upsampling, concatenation, the
 loss and Adam are plain PyTorch (device memory and autograd bookkeeping only).
 
-Training pairs (v, e) satisfy A e = v exactly: e is a smooth random complex field and v = A e is one FP64
-apply; the plane-wave solutions of each training model (v = b, e = A^-1 b) are added.  Models follow the
-C4 recipe: 64x64x16 cells of 100x100x50 m, log10 sigma ~ GRF(mean -2, std 0.8, correlation 200-800 m),
-frequency log-uniform in [1e-2, 1e1] Hz.
+Training pairs (v, e) satisfy A e = v exactly.  The default set comes from the solver's own Krylov
+histories (make_pairs_krylov): for each training model and plane-wave source, the outer FGMRES iterates
+x_k of a mixed-precision solve (k = 0 .. 6 outer iterations) give the residual r_k = b - A x_k and the error
+e_k = x* - x_k against a tight FP64 solution x*, so A e_k = r_k; these are the vectors the outer
+preconditioner sees during a solve.  An older set (make_pairs) uses smooth random fields e with v = A e and
+the plane-wave solutions.  Models follow the C4 recipe: 64x64x16 cells of 100x100x50 m,
+log10 sigma ~ GRF(mean -2, std 0.8, correlation 200-800 m), frequency log-uniform in [1e-2, 1e1] Hz.
 """
 from __future__ import annotations
 
@@ -237,6 +240,69 @@ def make_pairs(n_models=512, pairs_per_model=3, seed=0, solve_pairs=True, log=pr
     return torch.stack(X), torch.stack(Y)
 
 
+def _operator_system(m, sig, E0):
+    """SolveEquation's system (ie_solver_module.F90:62-80): A chi = rhs with rhs = sqrt(Re sigma_b) E0 and
+    E = a chi, a = 2 sqrt(Re sigma_b) / (csiga + conj sigma_b) per cell; returns (a, rhs) on the GPU."""
+    import torch
+    from .sources import _layer_numbers
+    from .synthetic import csiga_from_sigma
+    sb = m.csigma[_layer_numbers(m)[1:]]
+    sq = np.sqrt(sb.real)
+    a = 2.0 * sq[:, None, None] / (csiga_from_sigma(sig, m.freq) + np.conj(sb)[:, None, None])
+    rhs = sq[None, :, None, None] * E0
+    return torch.from_numpy(a).cuda(), torch.from_numpy(np.ascontiguousarray(rhs)).cuda()
+
+
+def make_pairs_krylov(n_models=512, max_k=6, seed=0, log=print):
+    """Residual/error pairs from the solver's own outer FGMRES histories on C4 models.
+
+    The outer iterate after k steps, x_k, is what a solve with an outer basis of k and one restart cycle
+    returns (the same Krylov space as the first k steps of the full solve); x_0 is the solver's start, the
+    right-hand side.  r_k = b - A x_k takes one FP64 apply, e_k = x* - x_k uses a tight FP64 solution x*."""
+    import torch
+    from .sources import plane_wave_integral
+    from .synthetic import config_c4
+    X, Y = [], []
+    t0 = time.perf_counter()
+    for i in range(n_models):
+        m, sig = config_c4(seed=seed * 100003 + i)
+        op = IEOperator.from_model(m)
+        op.calc_ie_kernel(m.csigma, m.thick, m.omega)
+        op.calc_fft_of_ie_kernel()
+        op.set_anomaly_sigma(sig, m.freq)
+        logsig, logf = model_features(m, sig)
+        E0 = plane_wave_integral(m, i % 2)
+        a, rhs = _operator_system(m, sig, E0)
+        b = torch.from_numpy(np.ascontiguousarray(E0).ravel()).cuda()
+        E = torch.empty_like(b)
+        ref = op.solve_device(b.data_ptr(), E.data_ptr(), None, tol=1e-10, precision=0)
+        if ref.stat != 1:
+            op.delete()
+            continue
+        xstar = E.view(3, *a.shape) / a
+        chis = [rhs]
+        for k in range(1, max_k + 1):
+            info = op.solve_device(b.data_ptr(), E.data_ptr(), None, tol=1e-14, max_restart=1, outer_buf=k,
+                                   precision=1)
+            chis.append(E.view(3, *a.shape) / a)
+            if info.iterations < k:
+                break
+        for chi in chis:
+            Ax = torch.empty_like(chi)
+            op.apply_device(chi.contiguous().data_ptr(), Ax.data_ptr(), 0)
+            r = rhs - Ax
+            e = xstar - chi
+            x, rms = encode(r, logsig, logf)
+            corr = (e - r) / rms
+            y = torch.stack([corr[c].real for c in range(3)] + [corr[c].imag for c in range(3)], dim=-1).float()
+            X.append(x[0].to(torch.bfloat16))
+            Y.append(y.to(torch.bfloat16))
+        op.delete()
+        if log and (i + 1) % 64 == 0:
+            log(f"Krylov pairs: {i + 1}/{n_models} models, {len(X)} pairs, {time.perf_counter() - t0:.1f} s")
+    return torch.stack(X), torch.stack(Y)
+
+
 def train(net, X, Y, steps=2000, batch=4, lr=1e-3, seed=0, log=print):
     """Adam on the relative squared error of the correction; returns the loss history."""
     import torch
@@ -345,7 +411,10 @@ def main(argv=None):
     import torch
     ap = argparse.ArgumentParser(description="train the learned outer preconditioner on C4 models")
     ap.add_argument("--models", type=int, default=512)
-    ap.add_argument("--pairs", type=int, default=3)
+    ap.add_argument("--pairs", type=int, default=3, help="smooth-field pairs per model (--data smooth)")
+    ap.add_argument("--data", default="krylov", choices=["krylov", "smooth"],
+                    help="training pairs: the solver's Krylov histories (default) or smooth random fields")
+    ap.add_argument("--max-k", type=int, default=6, help="outer iterates per model (--data krylov)")
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -362,7 +431,10 @@ def main(argv=None):
         print(json.dumps({"eval": rows}))
         return
     t0 = time.perf_counter()
-    X, Y = make_pairs(args.models, args.pairs, seed=1)
+    if args.data == "krylov":
+        X, Y = make_pairs_krylov(args.models, args.max_k, seed=1)
+    else:
+        X, Y = make_pairs(args.models, args.pairs, seed=1)
     t_data = time.perf_counter() - t0
     nval = max(8, X.shape[0] // 16)
     Xv, Yv = X[:nval], Y[:nval]
@@ -376,7 +448,7 @@ def main(argv=None):
     val = evaluate(net, Xv, Yv)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     net.save(args.out)
-    print(json.dumps({"pairs": int(X.shape[0]), "data_s": t_data, "train_s": t_train, "steps": args.steps,
+    print(json.dumps({"data": args.data, "pairs": int(X.shape[0]), "data_s": t_data, "train_s": t_train, "steps": args.steps,
                       "val_rel_err_untrained": base, "val_rel_err": val, "final_train_loss": float(np.mean(hist[-100:])),
                       "weights": args.out}))
 
