@@ -176,14 +176,17 @@ def test_hook_fallback_on_useless_guess(g2lib):
 
 
 def test_trained_network_gain(g2lib):
-    """What the committed, trained network gains on unseen C4 models: its guess of A^-1 v against the
-    guess z = v of the plain method, and the outer iterations of solves that use it."""
+    """What the committed network (trained on residual/error pairs of the solver's own outer Krylov
+    histories) gains on unseen C4 models: its guess of A^-1 r for the residuals of unseen solves against the
+    plain guess z = r, and the outer iterations of solves that use it.  Measured: the guess's error is a
+    fraction of the plain guess's, but the solves take as many outer iterations or more (the inner GMRES(10)
+    cycle is the stronger preconditioner), so the bounds below only hold the net to not breaking a solve."""
     import os
     import torch
-    from giem2g_b200.learned import WEIGHTS, LearnedPreconditioner, UNet3D, evaluate, make_pairs
+    from giem2g_b200.learned import WEIGHTS, LearnedPreconditioner, UNet3D, evaluate, make_pairs_krylov
     assert os.path.exists(WEIGHTS)
     net = UNet3D.from_file(WEIGHTS)
-    X, Y = make_pairs(n_models=2, pairs_per_model=2, seed=99, solve_pairs=False, log=None)
+    X, Y = make_pairs_krylov(n_models=2, max_k=3, seed=99, log=None)
     err = evaluate(net, X, Y)
     assert err < 0.5  # squared error of the correction, relative to the plain guess's (1.0)
     m, sig, op = _c4_op(g2lib, 903)
