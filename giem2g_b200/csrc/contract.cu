@@ -266,13 +266,14 @@ __global__ void __launch_bounds__(CfgT<R, NZ, S, B, NSTAGE, NP, SPLIT, MINB>::NT
 // s: each step sends half of the outputs a lane still holds to its partner and adds the half it
 // receives, so every lane ends with NR/SL of the NR = 2*3*PTS reals and stores them.  No CTA-wide
 // barrier is left in the consumer loop: one warp's reduction and stores overlap another's FMAs.
-template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB>
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, int VS = 1>
 struct CfgL {
     static constexpr int P = NZ * (NZ + 1) / 2;
     static constexpr int T = 4 * P + 2 * NZ * NZ;
     static constexpr int Z3 = 3 * NZ;
     static constexpr int PTS = 4 * NP;
-    static constexpr int ZW = 32 / SL;   // rows per warp
+    static constexpr int PL = LanePts<NP, VS>::PL;  // points per lane
+    static constexpr int ZW = 32 / (SL * VS);      // rows per warp
     static constexpr int W = NZ / ZW;    // warps per group
     static constexpr int NC = NG * W * 32;
     static constexpr int NTHREADS = NC + 32;
@@ -281,10 +282,10 @@ struct CfgL {
     static constexpr int TBYTES = T * ES;
     static constexpr int UBYTES = PTS * Z3 * ES;
     static constexpr int STAGE_BYTES = TBYTES + UBYTES;
-    static constexpr int NR = 2 * 3 * PTS;  // reals per lane before the reduction
+    static constexpr int NR = 2 * 3 * PL;   // reals per lane before the reduction
     static constexpr int HR = NR / SL;      // reals per lane after it
     static constexpr int SMEM = NSTAGE * STAGE_BYTES + 2 * NSTAGE * 8 + 16;  // + ticket counter
-    static_assert(32 % SL == 0 && NZ % ZW == 0, "slices must tile a warp and warps the rows");
+    static_assert(32 % (SL * VS) == 0 && NZ % ZW == 0, "slices x vector groups must tile a warp, warps the rows");
     static_assert(NR % SL == 0 && HR % 2 == 0, "every lane must end with whole complex outputs");
     static_assert(STAGE_BYTES % 16 == 0 && TBYTES % 16 == 0, "bulk copies need 16-byte multiples");
     static_assert(SMEM <= 232448, "exceeds the 227 KB dynamic shared memory of one CTA");
@@ -292,13 +293,14 @@ struct CfgL {
 };
 
 // PK (complex64): the packed 3-multiply form of k_contract_tma, two instructions per complex multiply-add.
-template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4, bool PK>
-__global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREADS, MINB)
+// VS: the NP vectors of a unit split over VS lane groups (LanePts): fewer points and registers per lane.
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4, bool PK, int VS = 1>
+__global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB, VS>::NTHREADS, MINB)
     k_contract_wl(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
                   long long nunits, int *err, const int *gate)
 {
     if (gate && *gate == 0) return;  // uniform across the CTA: nothing has been issued yet
-    using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>;
+    using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB, VS>;
     constexpr int PTS = Cfg::PTS, ZW = Cfg::ZW, W = Cfg::W;
     using C2 = typename V2<R>::T;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
     }
 
     const int warp = tid >> 5, lane = tid & 31;
-    const int g = warp / W, z = (warp % W) * ZW + lane % ZW, s = lane / ZW;
+    const int g = warp / W, z = (warp % W) * ZW + lane % ZW, s = (lane / ZW) % SL, vv = lane / (ZW * SL);
     for (long long it = g; it < my_n; it += NG) {
         const int slot = (int)(it % NSTAGE);
         const uint32_t round = (uint32_t)(it / NSTAGE);
@@ -364,12 +366,12 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>::NTHREAD
         const C2 *gb = reinterpret_cast<const C2 *>(st);
         const C2 *ub = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);  // [pt][c][j]
         R v[Cfg::NR];
-        wl_unit_sums<R, NZ, SL, NP, M4, PK>(gb, ub, z, s, v);
+        wl_unit_sums<R, NZ, SL, NP, M4, PK, VS>(gb, ub, z, s, v, vv);
         mbar_arrive(&empty[slot]);  // this lane's reads of the stage are done
 
         const long long unit = first + it * stride;
         const int q = (int)(unit / Ny), r = (int)(unit - (long long)q * Ny);
-        wl_unit_store<R, NZ, SL, NP>(v, s, q, r, Uhat + unit * PTS * Cfg::Z3 + z);
+        wl_unit_store<R, NZ, SL, NP, VS>(v, s, q, r, Uhat + unit * PTS * Cfg::Z3 + z, vv);
     }
 }
 
@@ -646,11 +648,12 @@ int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cud
     return G2_OK;
 }
 
-template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP = 1, int MINB = 1, bool M4 = false, bool PK = false>
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP = 1, int MINB = 1, bool M4 = false, bool PK = false,
+          int VS = 1>
 int launch_wl(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
-    using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB>;
-    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4, PK>;
+    using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB, VS>;
+    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4, PK, VS>;
     nsm *= MINB;
     static bool attr = false;
     if (!attr) {
@@ -772,7 +775,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 16 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 4 : 0); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 20 : ((Nz == 8 || Nz == 16 || Nz == 48) ? 4 : 0); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -804,6 +807,11 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         if (v == 13) return launch_wl<float, 32, 2, 3, 5, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 14) return launch_wl<float, 32, 2, 4, 5, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 15) return launch_wl<float, 32, 2, 5, 5, 2, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        // the two vectors split over lane groups: 4 points per lane
+        if (v == 16) return launch_wl<float, 32, 2, 3, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 17) return launch_wl<float, 32, 2, 4, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 18) return launch_wl<float, 32, 2, 2, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 19) return launch_wl<float, 32, 4, 2, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 32, 4, 2, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);

@@ -64,12 +64,25 @@ G2_D bool wait_ticket(const int *passed, int it, int *err, int code = 17)
     return true;
 }
 
-template <typename R, int NZ, int SL, int NP, bool M4, bool PK>
+// VS: the NP vectors split over VS lane groups (1: every lane holds all 4 NP points; NP: one vector per lane,
+// 4 points).  A lane of vector group vv holds the points (slot, vector vv * NP / VS + i); fewer points per lane
+// means fewer live accumulators and more resident warps, at the price of the tensor elements being read by
+// VS lanes instead of one.
+template <int NP, int VS> struct LanePts {
+    static_assert(NP % VS == 0, "the vector split must divide the vectors");
+    static constexpr int NPL = NP / VS;   // vectors per lane
+    static constexpr int PL = 4 * NPL;    // points per lane
+    // global point (slot * NP + vector) of the lane's local point p
+    static G2_HD int gp(int p, int vv) { return (p / NPL) * NP + vv * NPL + p % NPL; }
+};
+
+template <typename R, int NZ, int SL, int NP, bool M4, bool PK, int VS = 1>
 G2_D void wl_unit_sums(const typename V2<R>::T *__restrict__ gb, const typename V2<R>::T *__restrict__ ub, int z,
-                       int s, R (&v)[2 * 3 * 4 * NP])
+                       int s, R (&v)[2 * 3 * LanePts<NP, VS>::PL], int vv = 0)
 {
     using C2 = typename V2<R>::T;
-    constexpr int PTS = 4 * NP, P = NZ * (NZ + 1) / 2, JS = NZ / SL;
+    using LP = LanePts<NP, VS>;
+    constexpr int PTS = LP::PL, P = NZ * (NZ + 1) / 2, JS = NZ / SL;
     constexpr int AW = sizeof(R) == 8 ? asw_width64(NZ) : asw_width32(NZ);
     static_assert(!PK || (sizeof(R) == 4 && !M4), "packed pairs are a complex64 3-multiply form");
     constexpr int NA = M4 ? 2 : 3;
@@ -100,7 +113,7 @@ G2_D void wl_unit_sums(const typename V2<R>::T *__restrict__ gb, const typename 
         for (int p = 0; p < PTS; p++)
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                u[p][c] = ub[(p * 3 + c) * NZ + j];
+                u[p][c] = ub[(LP::gp(p, vv) * 3 + c) * NZ + j];
                 ue[p][c] = u[p][c].x + u[p][c].y;
             }
         // sign table as in k_contract_tma; point p = slot * NP + vector, slot bits (sx, m)
@@ -109,7 +122,7 @@ G2_D void wl_unit_sums(const typename V2<R>::T *__restrict__ gb, const typename 
     const R es_ = e[K].x + e[K].y;                                           \
     _Pragma("unroll") for (int p = 0; p < PTS; p++)                          \
     {                                                                        \
-        const int sl_ = p / NP;                                              \
+        const int sl_ = p / LP::NPL;                                         \
         const R sx = (sl_ & 2) ? R(-1) : R(1);                               \
         const R m = (sl_ & 1) ? R(-1) : R(1);                                \
         const R sg = (SGN);                                                  \
@@ -158,18 +171,20 @@ G2_D void wl_unit_sums(const typename V2<R>::T *__restrict__ gb, const typename 
         }
 }
 
-template <typename R, int NZ, int SL, int NP>
-G2_D void wl_unit_store(R (&v)[2 * 3 * 4 * NP], int s, int q, int r, typename V2<R>::T *dst)
+// lanes: zl + ZW * (s + SL * vv), ZW = 32 / (SL * VS) rows per warp
+template <typename R, int NZ, int SL, int NP, int VS = 1>
+G2_D void wl_unit_store(R (&v)[2 * 3 * LanePts<NP, VS>::PL], int s, int q, int r, typename V2<R>::T *dst, int vv = 0)
 {
     using C2 = typename V2<R>::T;
-    constexpr int PTS = 4 * NP, NR = 2 * 3 * PTS, HR = NR / SL, ZW = 32 / SL;
+    using LP = LanePts<NP, VS>;
+    constexpr int PTS = LP::PL, NR = 2 * 3 * PTS, HR = NR / SL, ZW = 32 / (SL * VS);
     int f0 = 0;  // first flat output index this lane keeps
     halve_slices<0, NR, ZW, SL, NR>(v, s, f0);
 #pragma unroll
     for (int i = 0; i < HR; i += 2) {
-        const int k = (f0 + i) >> 1, c = k / PTS, p = k - c * PTS, sl = p / NP;
+        const int k = (f0 + i) >> 1, c = k / PTS, p = k - c * PTS, sl = p / LP::NPL;
         C2 o{v[i], v[i + 1]};
         if ((q == 0 && (sl & 2)) || (r == 0 && (sl & 1))) o = C2{R(0), R(0)};
-        dst[(p * 3 + c) * NZ] = o;
+        dst[(LP::gp(p, vv) * 3 + c) * NZ] = o;
     }
 }

@@ -1,6 +1,6 @@
 """Model of the in-warp slice reduction of the barrier-free contraction (k_contract_wl, csrc/contract.cu).
 
-Lane = zl + ZW*s holds NR = 2*3*PTS partial sums (re, im of 3 components x PTS points) of row zl over
+Lane = zl + ZW*s (+ ZW*SL*vv when the vectors are split over lane groups) holds NR = 2*3*PTS partial sums (re, im of 3 components x PTS points) of row zl over
 its j-slice s. log2(SL) halving steps follow: at step b a lane whose bit b of s is set keeps the upper
 half of what it still holds and sends the lower half to lane ^ (ZW << b); the other lane does the
 opposite. Each adds what it receives to what it keeps. Afterwards lane s holds HR = NR/SL reals starting
@@ -26,7 +26,7 @@ def _halve(vals, SL, ZW):
         half = length // 2
         new = {}
         for lane in range(32):
-            s = lane // ZW
+            s = (lane // ZW) % SL
             up = (s >> b) & 1
             partner = lane ^ (ZW << b)
             mine = held[lane]
@@ -45,37 +45,45 @@ def _halve(vals, SL, ZW):
     return {lane: (f0[lane], held[lane][:length]) for lane in range(32)}
 
 
-# (SL, NP) of the shipped k_contract_wl shapes
-SHAPES = [(1, 1), (2, 1), (4, 1), (2, 2), (4, 2), (8, 2)]
+# (SL, NP, VS) of the shipped k_contract_wl shapes; VS > 1 splits the NP vectors over lane groups
+# (lane = zl + ZW*(s + SL*vv), ZW = 32/(SL*VS)), and a lane of group vv holds the LanePts points of its vectors
+SHAPES = [(1, 1, 1), (2, 1, 1), (4, 1, 1), (2, 2, 1), (4, 2, 1), (8, 2, 1), (2, 2, 2), (4, 2, 2)]
 
 
-@pytest.mark.parametrize("SL,NP", SHAPES)
-def test_halving_sums_every_output_once(SL, NP):
-    ZW = 32 // SL
-    PTS = 4 * NP
-    NR = 2 * 3 * PTS
+def _gp(p, vv, NP, VS):
+    """LanePts<NP, VS>::gp: the lane's local point p -> global point slot*NP + vector."""
+    npl = NP // VS
+    return (p // npl) * NP + vv * npl + p % npl
+
+
+@pytest.mark.parametrize("SL,NP,VS", SHAPES)
+def test_halving_sums_every_output_once(SL, NP, VS):
+    ZW = 32 // (SL * VS)
+    PL = 4 * NP // VS
+    NR = 2 * 3 * PL
     HR = NR // SL
     assert HR % 2 == 0  # whole complex outputs per lane (the kernel's static_assert)
-    rng = np.random.default_rng(SL * 10 + NP)
+    rng = np.random.default_rng(SL * 10 + NP + 100 * VS)
     vals = rng.standard_normal((32, NR))
     res = _halve(vals, SL, ZW)
     for zl in range(ZW):
-        lanes = [zl + ZW * s for s in range(SL)]
-        total = vals[lanes].sum(axis=0)  # the row's outputs summed over its slices
         stored = {}
-        for lane in lanes:
-            f0, kept = res[lane]
-            assert len(kept) == HR
-            np.testing.assert_allclose(kept, total[f0:f0 + HR], rtol=1e-12, atol=1e-12)
-            for i in range(0, HR, 2):
-                k = (f0 + i) >> 1
-                c, p = divmod(k, PTS)
-                assert (c, p) not in stored
-                stored[(c, p)] = (kept[i], kept[i + 1])
-        assert sorted(stored) == [(c, p) for c in range(3) for p in range(PTS)]
-        for (c, p), (re, im) in stored.items():
-            k = c * PTS + p
-            assert re == pytest.approx(total[2 * k]) and im == pytest.approx(total[2 * k + 1])
+        for vv in range(VS):
+            lanes = [zl + ZW * (s + SL * vv) for s in range(SL)]
+            total = vals[lanes].sum(axis=0)  # the row's outputs (this lane group's points) over its slices
+            for lane in lanes:
+                f0, kept = res[lane]
+                assert len(kept) == HR
+                np.testing.assert_allclose(kept, total[f0:f0 + HR], rtol=1e-12, atol=1e-12)
+                for i in range(0, HR, 2):
+                    k = (f0 + i) >> 1
+                    c, p = divmod(k, PL)
+                    key = (c, _gp(p, vv, NP, VS))
+                    assert key not in stored
+                    stored[key] = (kept[i], kept[i + 1])
+                    assert kept[i] == pytest.approx(total[2 * k]) and kept[i + 1] == pytest.approx(total[2 * k + 1])
+        # every (component, global point) of the row is stored exactly once across the lane groups
+        assert sorted(stored) == [(c, p) for c in range(3) for p in range(4 * NP)]
 
 
 def test_slices_of_one_lane_group_read_consecutive_j():
