@@ -729,7 +729,8 @@ def run_step_breakdown(args):
     for e in prof.events():
         if e.device_type != torch.autograd.DeviceType.CUDA:
             continue
-        name = e.name.split("<")[0].split("(")[0].replace("void ", "").replace("(anonymous namespace)::", "").strip()
+        name = e.name.replace("void ", "").replace("(anonymous namespace)::", "").replace("<unnamed>::", "")
+        name = name.split("<")[0].split("(")[0].strip()
         tot[name] += e.device_time_total
         cnt[name] += 1
         iv.append((e.time_range.start, e.time_range.end))

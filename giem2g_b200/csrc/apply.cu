@@ -26,6 +26,16 @@ template <typename R> using CT = typename Cplx<R>::T;
 
 constexpr int kThreads = 256;
 
+// Launch bounds of the FFT passes.  CAP = 0: any block up to 256 threads, registers as the compiler likes
+// (100-130 in FP64, 90-100 in complex64 at 2Ny = 256).  CAP = 1 holds more blocks per SM -- the passes are
+// latency-bound at 14-16 resident warps: complex64 at 64 registers (4 blocks of 256 threads), FP64 at 96
+// (5 blocks of 128 threads, so only for 8 lines per CTA).  Measured per apply at 128x128x32: complex64 passes
+// 88 -> 77 us, FP64 139 -> 128 us; tighter caps spill and lose.  Used for 2Ny, 2Nx <= 256 (the larger register
+// DFTs of longer lines do not fit the caps).
+template <typename R, int CAP> struct PassLB { static constexpr int T = kThreads, B = 1; };
+template <> struct PassLB<float, 1> { static constexpr int T = 256, B = 4; };
+template <> struct PassLB<double, 1> { static constexpr int T = 128, B = 5; };
+
 // The vectors of one apply: nv = 1, or nv = 2 right-hand sides of the same operator that share every
 // tensor read.  Line zc of a pass runs over [0, nv*3Nz): vector zc / 3Nz, row zc % 3Nz.
 template <typename C> struct VecSet {
@@ -57,8 +67,8 @@ G2_D void load_tw(C *dst, const C *__restrict__ src, int L)
 // ---------------------------------------------------------------------------------------------
 // k_fx: pre-scale by gsig, zero-pad to 2Nx, forward x-FFT.  CTA = one y row x NL (z,c) lines.
 // apply_ie_operator_module.F90:57-115 + Distributed_FFT.F90:552-569
-template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_fx(const VecSet<CT<R>> vs, const CT<R> *__restrict__ gsig,
+template <typename R, int L, int CAP>
+__global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_fx(const VecSet<CT<R>> vs, const CT<R> *__restrict__ gsig,
                                                  CT<R> *__restrict__ U1, const CT<R> *__restrict__ twg, int Nx,
                                                  int Ny, int Nz, int NL, const int *gate)
 {
@@ -86,8 +96,8 @@ __global__ void __launch_bounds__(kThreads) k_fx(const VecSet<CT<R>> vs, const C
 
 // k_fy: zero-pad to 2Ny, forward y-FFT of one kx column, scatter to (q, r, slot).
 // Distributed_FFT.F90:437-505 (y transform + +-ky repack) and :639-694 (+-kx repack)
-template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uh,
+template <typename R, int L, int CAP>
+__global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_fy(const CT<R> *__restrict__ U1, CT<R> *__restrict__ Uh,
                                                  const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
                                                  int nv, const int *gate)
 {
@@ -125,8 +135,8 @@ __global__ void __launch_bounds__(kThreads) k_fy(const CT<R> *__restrict__ U1, C
 }
 
 // k_by: inverse y-FFT of one kx column, crop y < Ny.  Distributed_FFT.F90:455-476, 696-788
-template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, CT<R> *__restrict__ U1,
+template <typename R, int L, int CAP>
+__global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_by(const CT<R> *__restrict__ Uh, CT<R> *__restrict__ U1,
                                                  const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
                                                  int nv, const int *gate)
 {
@@ -157,8 +167,8 @@ __global__ void __launch_bounds__(kThreads) k_by(const CT<R> *__restrict__ Uh, C
 
 // k_bx: inverse x-FFT, crop x < Nx, post-combine y = s*(a*x - w/(dz*4NxNy)).
 // apply_ie_operator_module.F90:125-174
-template <typename R, int L>
-__global__ void __launch_bounds__(kThreads) k_bx(const CT<R> *__restrict__ U1, const VecSet<CT<R>> vs,
+template <typename R, int L, int CAP>
+__global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_bx(const CT<R> *__restrict__ U1, const VecSet<CT<R>> vs,
                                                  const CT<R> *__restrict__ asig, const R *__restrict__ post,
                                                  const CT<R> *__restrict__ twg, int Nx, int Ny, int Nz, int NL,
                                                  const int *gate)
@@ -356,35 +366,56 @@ template <typename K> static void big_smem(K k)
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
+// the register-capped pass kernels apply when the block fits their bounds (PassLB)
+template <typename R, int L> static bool use_cap(int nt) { return L <= 256 && nt <= PassLB<R, 1>::T; }
+
+template <typename R, int L, int CAP>
+static void launch_x_k(bool fwd, IeOp *op, const VecSet<CT<R>> &vs, CT<R> *U1, cudaStream_t st, const int *gate,
+                       dim3 grid, int nt, size_t sm, int NL)
+{
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz;
+    static bool attr = false;
+    if (!attr) { big_smem(k_fx<R, L, CAP>); big_smem(k_bx<R, L, CAP>); attr = true; }
+    if (fwd)
+        k_fx<R, L, CAP><<<grid, nt, sm, st>>>(vs, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
+    else
+        k_bx<R, L, CAP><<<grid, nt, sm, st>>>(U1, vs, Bufs<R>::asig(op), Bufs<R>::post(op), Bufs<R>::twx(op), Nx,
+                                              Ny, Nz, NL, gate);
+}
+
 template <typename R, int L>
 static void launch_x(bool fwd, IeOp *op, const VecSet<CT<R>> &vs, CT<R> *U1, cudaStream_t st, const int *gate)
 {
-    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = vs.nv * 3 * Nz;
+    const int Nz = op->Nz, ZL = vs.nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
     const int NL = lines_for(L, es, op->fft_lines[es == sizeof(double2) ? 0 : 1]), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
-    dim3 grid((ZL + NL - 1) / NL, Ny);
+    dim3 grid((ZL + NL - 1) / NL, op->Ny);
+    if (use_cap<R, L>(nt)) launch_x_k<R, L, 1>(fwd, op, vs, U1, st, gate, grid, nt, sm, NL);
+    else launch_x_k<R, L, 0>(fwd, op, vs, U1, st, gate, grid, nt, sm, NL);
+}
+
+template <typename R, int L, int CAP>
+static void launch_y_k(bool fwd, IeOp *op, int nv, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate,
+                       dim3 grid, int nt, size_t sm, int NL)
+{
+    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz;
     static bool attr = false;
-    if (!attr) { big_smem(k_fx<R, L>); big_smem(k_bx<R, L>); attr = true; }
-    if (fwd)
-        k_fx<R, L><<<grid, nt, sm, st>>>(vs, Bufs<R>::gsig(op), U1, Bufs<R>::twx(op), Nx, Ny, Nz, NL, gate);
-    else
-        k_bx<R, L><<<grid, nt, sm, st>>>(U1, vs, Bufs<R>::asig(op), Bufs<R>::post(op), Bufs<R>::twx(op), Nx, Ny,
-                                         Nz, NL, gate);
+    if (!attr) { big_smem(k_fy<R, L, CAP>); big_smem(k_by<R, L, CAP>); attr = true; }
+    if (fwd) k_fy<R, L, CAP><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL, nv, gate);
+    else k_by<R, L, CAP><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL, nv, gate);
 }
 
 template <typename R, int L>
 static void launch_y(bool fwd, IeOp *op, int nv, CT<R> *U1, CT<R> *Uh, cudaStream_t st, const int *gate)
 {
-    const int Nx = op->Nx, Ny = op->Ny, Nz = op->Nz, ZL = nv * 3 * Nz;
+    const int Nz = op->Nz, ZL = nv * 3 * Nz;
     const size_t es = sizeof(CT<R>);
     const int NL = lines_for(L, es, op->fft_lines[es == sizeof(double2) ? 0 : 1]), nt = threads_for(L, NL);
     const size_t sm = (size_t)(NL * (L + 1) + L) * es;
-    dim3 grid((ZL + NL - 1) / NL, 2 * Nx);
-    static bool attr = false;
-    if (!attr) { big_smem(k_fy<R, L>); big_smem(k_by<R, L>); attr = true; }
-    if (fwd) k_fy<R, L><<<grid, nt, sm, st>>>(U1, Uh, Bufs<R>::twy(op), Nx, Ny, Nz, NL, nv, gate);
-    else k_by<R, L><<<grid, nt, sm, st>>>(Uh, U1, Bufs<R>::twy(op), Nx, Ny, Nz, NL, nv, gate);
+    dim3 grid((ZL + NL - 1) / NL, 2 * op->Nx);
+    if (use_cap<R, L>(nt)) launch_y_k<R, L, 1>(fwd, op, nv, U1, Uh, st, gate, grid, nt, sm, NL);
+    else launch_y_k<R, L, 0>(fwd, op, nv, U1, Uh, st, gate, grid, nt, sm, NL);
 }
 
 template <typename R>
