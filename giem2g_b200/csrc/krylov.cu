@@ -16,6 +16,7 @@
 // The inner solver's closing true-residual apply (gmres.F90:403) produces a number nobody reads; it
 // is skipped unless the environment variable GIEM2G_INNER_TRUE_RESIDUAL=1 asks for it (the solution
 // and iteration history are the same either way; only the apply count differs).
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -1148,10 +1149,12 @@ int krylov_history(IeOp *op, double *out, int max_len)
 // device flag and the host stops launching their outer work.
 namespace {
 
-__global__ void k_set_bn_masked(Level L, const int *active)
+// outer_go: the instance's outer Krylov flag (F_KRYLOV of its outer level); an inner cycle enqueued after the
+// instance converged (one outer step ahead of the host, see batch_outer) does nothing
+__global__ void k_set_bn_masked(Level L, const int *active, const int *outer_go)
 {
     L.scal[S_BN] = sqrt(L.scal[S_NRM2]);
-    L.flags[F_SOLVER] = (L.scal[S_BN] < ZERO_THRESHOLD || *active == 0) ? 0 : 1;
+    L.flags[F_SOLVER] = (L.scal[S_BN] < ZERO_THRESHOLD || *active == 0 || *outer_go == 0) ? 0 : 1;
     L.flags[F_ITER] = 0;
     L.flags[F_KRYLOV] = L.flags[F_SOLVER];
     L.flags[F_L] = 0;
@@ -1173,6 +1176,10 @@ struct BatchWork {
     int *d_active = nullptr;
     std::vector<int> h_active, dev_active;  // host mask and its copy on the device
     double2 *d_stage = nullptr;  // host-array solves: E_bkg[n] then E_sol[n] (complex128)
+    // pinned host copies of the outer levels' scalars and flags, two slots (outer step j uses slot j % 2),
+    // each completed by its own event
+    void *h_pin = nullptr;
+    cudaEvent_t ev_pull[2] = {nullptr, nullptr};
     cudaStream_t st = nullptr;
     // One captured inner cycle per mask of active instances: a solve changes the mask as instances
     // converge, and the next solve starts from all-active again, so the graphs are kept, not re-captured.
@@ -1195,6 +1202,9 @@ static void batch_destroy(BatchWork *b)
     for (auto &gr : b->graphs)
         if (gr.exec) cudaGraphExecDestroy(gr.exec);
     for (KrylovWork *k : b->k) kw_free(k);
+    if (b->h_pin) cudaFreeHost(b->h_pin);
+    for (cudaEvent_t e : b->ev_pull)
+        if (e) cudaEventDestroy(e);
     if (b->d_active) cudaFree(b->d_active);
     if (b->d_stage) cudaFree(b->d_stage);
     delete b;
@@ -1295,7 +1305,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         const int g = vec_grid(k->N);
         k_zero_level<<<1, 256, 0, st>>>(L); g2_count_launches(1);
         norm2<CI>(k, reinterpret_cast<const CI *>(k->vin), L.scal + S_NRM2, b->d_active + i, st);
-        k_set_bn_masked<<<1, 1, 0, st>>>(L, b->d_active + i); g2_count_launches(1);
+        k_set_bn_masked<<<1, 1, 0, st>>>(L, b->d_active + i, k->Lo.flags + F_KRYLOV); g2_count_launches(1);
         k_copy_or_zero<CI><<<g, kVT, 0, st>>>(reinterpret_cast<CI *>(k->xin), reinterpret_cast<const CI *>(k->vin),
                                              L.scal, k->N); g2_count_launches(1);
     }
@@ -1463,6 +1473,32 @@ static int batch_pull(BatchWork *b, std::vector<BatchScal> &h, cudaStream_t st)
     return G2_OK;
 }
 
+// The same copies into pinned slot `slot`, completed by an event instead of a synchronisation, so the host can
+// enqueue more work before it waits (batch_outer's outer step j + 1).
+static int batch_pull_async(BatchWork *b, int slot, cudaStream_t st)
+{
+    if (!b->h_pin) {
+        G2_CUDA_CHECK(cudaMallocHost(&b->h_pin, 2 * sizeof(BatchScal) * b->n));
+        for (cudaEvent_t &e : b->ev_pull) G2_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    BatchScal *h = reinterpret_cast<BatchScal *>(b->h_pin) + (size_t)slot * b->n;
+    for (int i = 0; i < b->n; i++) {
+        if (!b->h_active[i]) continue;
+        G2_CUDA_CHECK(cudaMemcpyAsync(h[i].s, b->k[i]->Lo.scal, sizeof(h[i].s), cudaMemcpyDeviceToHost, st));
+        G2_CUDA_CHECK(cudaMemcpyAsync(h[i].f, b->k[i]->Lo.flags, sizeof(h[i].f), cudaMemcpyDeviceToHost, st));
+    }
+    G2_CUDA_CHECK(cudaEventRecord(b->ev_pull[slot], st));
+    return G2_OK;
+}
+static int batch_pull_wait(BatchWork *b, int slot, std::vector<BatchScal> &h)
+{
+    G2_CUDA_CHECK(cudaEventSynchronize(b->ev_pull[slot]));
+    const BatchScal *p = reinterpret_cast<const BatchScal *>(b->h_pin) + (size_t)slot * b->n;
+    for (int i = 0; i < b->n; i++)
+        if (b->h_active[i]) h[i] = p[i];
+    return G2_OK;
+}
+
 // FinalActions of instance i (gmres.F90:382-421) after the host learned that it stops
 template <typename CI>
 static void batch_final_launch(BatchWork *b, int i, cudaStream_t st, int &rc)
@@ -1544,32 +1580,64 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
             k_scale_by<double2><<<vec_grid(k->N), kVT, 0, st>>>(k->Vo, k->w, k->Lo.scal, S_BETA, k->N, nullptr); g2_count_launches(1);
         }
         bool cycle_done = false;
-        for (int j = 0; j < M && !cycle_done; j++) {
+        // Outer step j of every active instance.  Its kernels are gated by the instance's outer Krylov flag,
+        // which the Arnoldi tail of step j - 1 clears when the instance converged (or its cycle ended): step
+        // j + 1 is enqueued before the host reads step j's misfits, so the GPU does not wait for the host
+        // between steps, and an instance that converged at step j does nothing in step j + 1.  The arithmetic
+        // of the instances that go on is unchanged.
+        auto enqueue_step = [&](int j) -> int {
             for (int i = 0; i < n; i++) {
                 if (!b->h_active[i]) continue;
                 KrylovWork *k = b->k[i];
+                const int *go = k->Lo.flags + F_KRYLOV;
                 k_axpby<CI, double2, double2><<<vec_grid(k->N), kVT, 0, st>>>(
                     reinterpret_cast<CI *>(k->vin), 1.0, k->Vo + (size_t)j * k->N, 0.0, (const double2 *)nullptr, k->N,
-                    nullptr); g2_count_launches(1);
+                    go); g2_count_launches(1);
             }
-            if ((rc = batch_inner_fixed<CI>(b, tol, st))) return rc;
+            int r = batch_inner_fixed<CI>(b, tol, st);
+            if (r) return r;
             for (int i = 0; i < n; i++) {
                 if (!b->h_active[i]) continue;
                 KrylovWork *k = b->k[i];
                 const int g = vec_grid(k->N);
+                const int *go = k->Lo.flags + F_KRYLOV;
                 CI *Zj = reinterpret_cast<CI *>(k->Zo) + (size_t)j * k->N;
-                k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, k->N, nullptr); g2_count_launches(1);
+                k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
                 if (sizeof(CI) == sizeof(double2)) {
-                    if ((rc = ie_apply_device64(b->ops[i], reinterpret_cast<const double2 *>(Zj), k->w, st))) return rc;
+                    if ((r = ie_apply_device64(b->ops[i], reinterpret_cast<const double2 *>(Zj), k->w, st, go))) return r;
                 } else {
-                    k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, k->N, nullptr); g2_count_launches(1);
-                    if ((rc = ie_apply_device64(b->ops[i], k->tmp, k->w, st))) return rc;
+                    k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
+                    if ((r = ie_apply_device64(b->ops[i], k->tmp, k->w, st, go))) return r;
                 }
-                k->applies64++;
-                cgs<double2>(k, k->Lo, k->Vo, j, k->w, nullptr, st);
-                arnoldi_tail<double2>(k, k->Lo, k->Vo, j, k->w, tol, nullptr, st);
+                cgs<double2>(k, k->Lo, k->Vo, j, k->w, go, st);
+                arnoldi_tail<double2>(k, k->Lo, k->Vo, j, k->w, tol, go, st);
             }
-            if ((rc = batch_pull(b, h, st))) return rc;
+            return G2_OK;
+        };
+        // Running ahead is skipped when an instance is expected to converge at step j (its last misfit times
+        // its last reduction factor within kAheadMargin of the tolerance): a step enqueued after that keeps the
+        // pair's shared complex64 applies for an instance that would otherwise run its single applies.
+        auto near_tol = [&]() {
+            constexpr double kAheadMargin = 4.0;
+            for (int i = 0; i < n; i++) {
+                if (!b->h_active[i] || b->history[i].empty()) continue;
+                const std::vector<double> &hs = b->history[i];
+                const double last = hs.back();
+                const double r = hs.size() > 1 && hs[hs.size() - 2] > 0.0 ? std::min(1.0, last / hs[hs.size() - 2]) : 1.0;
+                if (last * r < kAheadMargin * tol) return true;
+            }
+            return false;
+        };
+        bool ahead = false;  // step j was enqueued ahead, during step j - 1
+        for (int j = 0; j < M && !cycle_done; j++) {
+            if (!ahead && (rc = enqueue_step(j))) return rc;
+            if ((rc = batch_pull_async(b, j & 1, st))) return rc;
+            ahead = j + 1 < M && !near_tol();
+            if (ahead && (rc = enqueue_step(j + 1))) return rc;
+            if ((rc = batch_pull_wait(b, j & 1, h))) return rc;
+            // an instance still active here ran step j (it had not converged at step j - 1)
+            for (int i = 0; i < n; i++)
+                if (b->h_active[i]) b->k[i]->applies64++;
             for (int i = 0; i < n; i++) {
                 if (!b->h_active[i]) continue;
                 bea[i] = h[i].s[S_BEA];
