@@ -59,6 +59,39 @@ template <typename C> G2_D void st2(C *p, size_t i, double2 v);
 template <> G2_D void st2<double2>(double2 *p, size_t i, double2 v) { p[i] = v; }
 template <> G2_D void st2<float2>(float2 *p, size_t i, double2 v) { p[i] = make_float2((float)v.x, (float)v.y); }
 
+// The basis sweeps move 16-byte words: two complex64 values per load (complex128 values are 16 bytes
+// already).  On a B200 a two-instance sweep of 11 complex64 vectors of 1.57 M elements took 84 us with
+// 8-byte loads and 52 us with 16-byte loads.  Vectors whose length (and column stride) is odd keep
+// element-wise loads, since their odd columns are not 16-byte aligned.
+template <typename C> struct Wide;
+template <> struct Wide<float2> {
+    using T = float4;
+    static constexpr int E = 2;
+};
+template <> struct Wide<double2> {
+    using T = double2;
+    static constexpr int E = 1;
+};
+G2_D float2 part_of(const float4 &p, int e) { return e ? make_float2(p.z, p.w) : make_float2(p.x, p.y); }
+G2_D double2 part_of(const double2 &p, int) { return p; }
+G2_D void set_part(float4 &p, int e, float2 v)
+{
+    if (e) {
+        p.z = v.x;
+        p.w = v.y;
+    } else {
+        p.x = v.x;
+        p.y = v.y;
+    }
+}
+G2_D void set_part(double2 &p, int, double2 v) { p = v; }
+// words of E elements over the whole vector, or 0 when the lengths do not allow them
+template <typename C> G2_D size_t wide_words(size_t N, size_t ld)
+{
+    constexpr int E = Wide<C>::E;
+    return (N % E == 0 && ld % E == 0) ? N / E : 0;
+}
+
 template <typename C> struct RealOf;
 template <> struct RealOf<double2> { using T = double; };
 template <> struct RealOf<float2> { using T = float; };
@@ -193,21 +226,17 @@ G2_D void reduce_partials(const double2 *part, int nb, int K, double2 *h, double
     for (int k = warp; k <= K; k += nw) {
         const int col = (k == K) ? KMAX : k;
         double sx = 0.0, sy = 0.0;
-        // four independent loads per lane and round: the partials come from L2, and a chain of dependent
-        // loads (one per 32 blocks) made this tail cost several microseconds per reduction
-        int b = lane;
-        for (; b + 96 < nb; b += 128) {
-            const double2 v0 = __ldcg(part + (size_t)b * (KMAX + 1) + col);
-            const double2 v1 = __ldcg(part + (size_t)(b + 32) * (KMAX + 1) + col);
-            const double2 v2 = __ldcg(part + (size_t)(b + 64) * (KMAX + 1) + col);
-            const double2 v3 = __ldcg(part + (size_t)(b + 96) * (KMAX + 1) + col);
-            sx += (v0.x + v1.x) + (v2.x + v3.x);
-            sy += (v0.y + v1.y) + (v2.y + v3.y);
-        }
-        for (; b < nb; b += 32) {
-            const double2 v = __ldcg(part + (size_t)b * (KMAX + 1) + col);
-            sx += v.x;
-            sy += v.y;
+        // eight independent loads per lane and round (rows past nb predicated off): the partials come from
+        // L2, and each round is one L2 round trip, so 256 rows cost one
+        for (int b0 = 0; b0 < nb; b0 += 256) {
+            double2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const int b = b0 + lane + 32 * q;
+                v[q] = b < nb ? __ldcg(part + (size_t)b * (KMAX + 1) + col) : make_double2(0.0, 0.0);
+            }
+            sx += ((v[0].x + v[1].x) + (v[2].x + v[3].x)) + ((v[4].x + v[5].x) + (v[6].x + v[7].x));
+            sy += ((v[0].y + v[1].y) + (v[2].y + v[3].y)) + ((v[4].y + v[5].y) + (v[6].y + v[7].y));
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -236,29 +265,52 @@ G2_D void dots_first_body(const C *__restrict__ V, size_t ld, const C *__restric
                           Level &L)
 {
     using R = typename RealOf<C>::T;
-    constexpr int U = SweepU<K, C>::v > 0 ? SweepU<K, C>::v : 1;
+    using W = typename Wide<C>::T;
+    constexpr int E = Wide<C>::E;
+    constexpr int U = SweepU<K, W>::v > 0 ? SweepU<K, W>::v : 1;
     R ax[K + 1], ay[K + 1];
 #pragma unroll
     for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
-    const size_t S = (size_t)gridDim.x * kVT;
-    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
-    for (; SweepU<K, C>::v > 0 && i + (U - 1) * S < N; i += U * S) {
-        C wv[U], v[K > 0 ? K : 1][U];
+    const size_t S = (size_t)gridDim.x * kVT, t0 = blockIdx.x * (size_t)kVT + threadIdx.x;
+    const size_t Nw = wide_words<C>(N, ld), ldw = ld / E;
+    const W *__restrict__ Vw = reinterpret_cast<const W *>(V);
+    const W *__restrict__ ww = reinterpret_cast<const W *>(w);
+    size_t i = t0;
+    for (; SweepU<K, W>::v > 0 && i + (U - 1) * S < Nw; i += U * S) {
+        W wv[U], v[K > 0 ? K : 1][U];
 #pragma unroll
-        for (int u = 0; u < U; u++) wv[u] = w[i + u * S];
+        for (int u = 0; u < U; u++) wv[u] = ww[i + u * S];
 #pragma unroll
         for (int k = 0; k < K; k++)
 #pragma unroll
-            for (int u = 0; u < U; u++) v[k][u] = V[(size_t)k * ld + i + u * S];
+            for (int u = 0; u < U; u++) v[k][u] = Vw[(size_t)k * ldw + i + u * S];
 #pragma unroll
         for (int u = 0; u < U; u++)
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                ax[k] += v[k][u].x * wv[u].x + v[k][u].y * wv[u].y;
-                ay[k] += v[k][u].x * wv[u].y - v[k][u].y * wv[u].x;
+            for (int e = 0; e < E; e++) {
+                const C a = part_of(wv[u], e);
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const C b = part_of(v[k][u], e);
+                    ax[k] += b.x * a.x + b.y * a.y;
+                    ay[k] += b.x * a.y - b.y * a.x;
+                }
             }
     }
-    for (; i < N; i += S) {
+    for (; i < Nw; i += S) {
+        const W wv = ww[i];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const W v = Vw[(size_t)k * ldw + i];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const C a = part_of(wv, e), b = part_of(v, e);
+                ax[k] += b.x * a.x + b.y * a.y;
+                ay[k] += b.x * a.y - b.y * a.x;
+            }
+        }
+    }
+    for (i = Nw * E + t0; i < N; i += S) {
         const C wv = w[i];
 #pragma unroll
         for (int k = 0; k < K; k++) {
@@ -308,6 +360,8 @@ G2_D void cgs_pass_body(const C *__restrict__ V, size_t ld, C *__restrict__ w, s
                         int p)
 {
     using R = typename RealOf<C>::T;
+    using W = typename Wide<C>::T;
+    constexpr int E = Wide<C>::E;
     constexpr int KA = K > 0 ? K : 1;
     __shared__ double2 hsh[KA];
     if (threadIdx.x < K) hsh[threadIdx.x] = L.hpass[threadIdx.x];
@@ -315,36 +369,83 @@ G2_D void cgs_pass_body(const C *__restrict__ V, size_t ld, C *__restrict__ w, s
     R ax[K + 1], ay[K + 1];
 #pragma unroll
     for (int k = 0; k <= K; k++) ax[k] = ay[k] = R(0);
-    constexpr int U = SweepU<K, C>::v > 0 ? SweepU<K, C>::v : 1;
-    const size_t S = (size_t)gridDim.x * kVT;
-    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
-    // U elements per round, every load of the round first; the basis values stay in registers for the dots
-    for (; SweepU<K, C>::v > 0 && i + (U - 1) * S < N; i += U * S) {
-        C wv[U], v[K > 0 ? K : 1][U];
+    constexpr int U = SweepU<K, W>::v > 0 ? SweepU<K, W>::v : 1;
+    const size_t S = (size_t)gridDim.x * kVT, t0 = blockIdx.x * (size_t)kVT + threadIdx.x;
+    const size_t Nw = wide_words<C>(N, ld), ldw = ld / E;
+    const W *__restrict__ Vw = reinterpret_cast<const W *>(V);
+    W *__restrict__ ww = reinterpret_cast<W *>(w);
+    // one element: w -= V hpass, then |w|^2 and the dots of the new w (the basis values stay in registers)
+    auto element = [&](C &a, const C *b) {
 #pragma unroll
-        for (int u = 0; u < U; u++) wv[u] = w[i + u * S];
+        for (int k = 0; k < K; k++) {
+            const R hx = (R)hsh[k].x, hy = (R)hsh[k].y;
+            a.x -= b[k].x * hx - b[k].y * hy;
+            a.y -= b[k].x * hy + b[k].y * hx;
+        }
+        ax[K] += a.x * a.x + a.y * a.y;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            ax[k] += b[k].x * a.x + b[k].y * a.y;
+            ay[k] += b[k].x * a.y - b[k].y * a.x;
+        }
+    };
+    size_t i = t0;
+    // U words per round, every load of the round first
+    for (; SweepU<K, W>::v > 0 && i + (U - 1) * S < Nw; i += U * S) {
+        W wv[U], v[K > 0 ? K : 1][U];
+#pragma unroll
+        for (int u = 0; u < U; u++) wv[u] = ww[i + u * S];
 #pragma unroll
         for (int k = 0; k < K; k++)
 #pragma unroll
-            for (int u = 0; u < U; u++) v[k][u] = V[(size_t)k * ld + i + u * S];
+            for (int u = 0; u < U; u++) v[k][u] = Vw[(size_t)k * ldw + i + u * S];
 #pragma unroll
         for (int u = 0; u < U; u++) {
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                const R hx = (R)hsh[k].x, hy = (R)hsh[k].y;
-                wv[u].x -= v[k][u].x * hx - v[k][u].y * hy;
-                wv[u].y -= v[k][u].x * hy + v[k][u].y * hx;
-            }
-            w[i + u * S] = wv[u];
-            ax[K] += wv[u].x * wv[u].x + wv[u].y * wv[u].y;
+            for (int e = 0; e < E; e++) {
+                C a = part_of(wv[u], e), b[K > 0 ? K : 1];
 #pragma unroll
-            for (int k = 0; k < K; k++) {
-                ax[k] += v[k][u].x * wv[u].x + v[k][u].y * wv[u].y;
-                ay[k] += v[k][u].x * wv[u].y - v[k][u].y * wv[u].x;
+                for (int k = 0; k < K; k++) b[k] = part_of(v[k][u], e);
+                element(a, b);
+                set_part(wv[u], e, a);
+            }
+            ww[i + u * S] = wv[u];
+        }
+    }
+    // the rest (all of it when the basis is too wide to hold): one word at a time, the basis read twice
+    for (; i < Nw; i += S) {
+        W wv = ww[i];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const W v = Vw[(size_t)k * ldw + i];
+            const R hx = (R)hsh[k].x, hy = (R)hsh[k].y;
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                C a = part_of(wv, e);
+                const C b = part_of(v, e);
+                a.x -= b.x * hx - b.y * hy;
+                a.y -= b.x * hy + b.y * hx;
+                set_part(wv, e, a);
+            }
+        }
+        ww[i] = wv;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const C a = part_of(wv, e);
+            ax[K] += a.x * a.x + a.y * a.y;
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const W v = Vw[(size_t)k * ldw + i];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const C a = part_of(wv, e), b = part_of(v, e);
+                ax[k] += b.x * a.x + b.y * a.y;
+                ay[k] += b.x * a.y - b.y * a.x;
             }
         }
     }
-    for (; i < N; i += S) {
+    for (i = Nw * E + t0; i < N; i += S) {
         C wv = w[i];
 #pragma unroll
         for (int k = 0; k < K; k++) {
@@ -410,24 +511,41 @@ __global__ void __launch_bounds__(kVT) k_norm2_fused(const C *__restrict__ w, si
 }
 
 // end of Arnoldi step j: V_{j+1} = w / ||w||, then the last block runs the Givens/misfit step
+G2_D float2 scaled(float2 a, double s) { return make_float2((float)(a.x * s), (float)(a.y * s)); }
+G2_D double2 scaled(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+G2_D double2 widen(float2 a) { return make_double2(a.x, a.y); }
+G2_D double2 widen(double2 a) { return a; }
+
 template <typename C>
 G2_D void scale_finish_body(C *v, const C *w, size_t N, Level &L, int j, double tol)
 {
+    using W = typename Wide<C>::T;
+    constexpr int E = Wide<C>::E;
     const double inv = 1.0 / L.scal[S_DNORMW];
-    // kILP independent elements per thread and iteration, loads first: more bytes in flight per SM
-    const size_t S = (size_t)gridDim.x * kVT;
-    size_t i = blockIdx.x * (size_t)kVT + threadIdx.x;
-    for (; i + (kILP - 1) * S < N; i += kILP * S) {
-        double2 x[kILP];
+    // kILP independent words per thread and iteration, loads first: more bytes in flight per SM
+    const size_t S = (size_t)gridDim.x * kVT, t0 = blockIdx.x * (size_t)kVT + threadIdx.x;
+    const size_t Nw = wide_words<C>(N, N);
+    const W *__restrict__ ww = reinterpret_cast<const W *>(w);
+    W *__restrict__ vw = reinterpret_cast<W *>(v);
+    size_t i = t0;
+    for (; i + (kILP - 1) * S < Nw; i += kILP * S) {
+        W x[kILP];
 #pragma unroll
-        for (int u = 0; u < kILP; u++) x[u] = ld2(w, i + u * S);
+        for (int u = 0; u < kILP; u++) x[u] = ww[i + u * S];
 #pragma unroll
-        for (int u = 0; u < kILP; u++) st2(v, i + u * S, make_double2(x[u].x * inv, x[u].y * inv));
+        for (int u = 0; u < kILP; u++) {
+#pragma unroll
+            for (int e = 0; e < E; e++) set_part(x[u], e, scaled(part_of(x[u], e), inv));
+            vw[i + u * S] = x[u];
+        }
     }
-    for (; i < N; i += S) {
-        const double2 x = ld2(w, i);
-        st2(v, i, make_double2(x.x * inv, x.y * inv));
+    for (; i < Nw; i += S) {
+        W x = ww[i];
+#pragma unroll
+        for (int e = 0; e < E; e++) set_part(x, e, scaled(part_of(x, e), inv));
+        vw[i] = x;
     }
+    for (i = Nw * E + t0; i < N; i += S) v[i] = scaled(w[i], inv);
     if (!last_block(L.counter)) return;
     if (threadIdx.x == 0) arnoldi_finish_body(L, j, tol);
 }
@@ -577,7 +695,50 @@ __global__ void __launch_bounds__(kVT) k_lincomb(CO *out, double a0, const CO *i
     const int n = *nflag;
     if (threadIdx.x < n) cs[threadIdx.x] = coef[threadIdx.x];
     __syncthreads();
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+    using W = typename Wide<CB>::T;
+    constexpr int E = Wide<CB>::E;
+    constexpr int KU = 4;  // basis words loaded together
+    const size_t S = (size_t)gridDim.x * kVT, t0 = blockIdx.x * (size_t)kVT + threadIdx.x;
+    const size_t Nw = wide_words<CB>(N, ld), ldw = ld / E;
+    const W *__restrict__ Bw = reinterpret_cast<const W *>(Bm);
+    size_t i = t0;
+    for (; i < Nw; i += S) {
+        double2 r[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            r[e] = make_double2(0.0, 0.0);
+            if (in0) {
+                const double2 x = ld2(in0, i * E + e);
+                r[e] = make_double2(a0 * x.x, a0 * x.y);
+            }
+        }
+        int k = 0;
+        for (; k + KU <= n; k += KU) {
+            W v[KU];
+#pragma unroll
+            for (int q = 0; q < KU; q++) v[q] = Bw[(size_t)(k + q) * ldw + i];
+#pragma unroll
+            for (int q = 0; q < KU; q++)
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    const double2 b = widen(part_of(v[q], e)), c = cs[k + q];
+                    r[e].x += b.x * c.x - b.y * c.y;
+                    r[e].y += b.x * c.y + b.y * c.x;
+                }
+        }
+        for (; k < n; k++) {
+            const W v = Bw[(size_t)k * ldw + i];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const double2 b = widen(part_of(v, e)), c = cs[k];
+                r[e].x += b.x * c.x - b.y * c.y;
+                r[e].y += b.x * c.y + b.y * c.x;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) st2(out, i * E + e, r[e]);
+    }
+    for (i = Nw * E + t0; i < N; i += S) {
         double2 r = make_double2(0.0, 0.0);
         if (in0) {
             const double2 x = ld2(in0, i);
@@ -633,6 +794,13 @@ int vec_grid(size_t N)
     const size_t need = (N + kVT - 1) / kVT;
     const size_t g = (size_t)sms * 4;
     return (int)(need < g ? need : g);
+}
+// blocks of the sweeps that end in a last-block reduction: two per SM and instance streamed as fast as
+// four in the basis sweeps, and leave the last block half as many partial sums to add
+int sweep_grid(size_t N)
+{
+    const int g = vec_grid(N);
+    return g > 8 ? (g + 1) / 2 : g;
 }
 
 }  // namespace
@@ -729,7 +897,7 @@ static int kw_alloc(KrylovWork *k, size_t N, int mo, int mi, int precision)
     G2_CUDA_CHECK(cudaMalloc(&k->vin, ei * N));
     G2_CUDA_CHECK(cudaMalloc(&k->xin, ei * N));
     G2_CUDA_CHECK(cudaMalloc(&k->x0in, ei * N));
-    k->nparts = vec_grid(N);
+    k->nparts = sweep_grid(N);
     G2_CUDA_CHECK(cudaMalloc(&k->part, sizeof(double2) * (size_t)k->nparts * (KMAX + 1)));
     int rc = alloc_level(k->Lo, mo);
     if (!rc) rc = alloc_level(k->Li, mi);
@@ -802,7 +970,7 @@ static void cgs(KrylovWork *k, Level &L, const C *V, int j, C *w, const int *gat
 template <typename C>
 static void arnoldi_tail(KrylovWork *k, Level &L, C *V, int j, const C *w, double tol, const int *gate, cudaStream_t st)
 {
-    k_scale_finish<C><<<vec_grid(k->N), kVT, 0, st>>>(V + (size_t)(j + 1) * k->N, w, k->N, L, j, tol, gate);
+    k_scale_finish<C><<<sweep_grid(k->N), kVT, 0, st>>>(V + (size_t)(j + 1) * k->N, w, k->N, L, j, tol, gate);
     g2_count_launches(1);
 }
 
@@ -832,7 +1000,7 @@ static void cgs_multi(const Multi<C> &mm, int n, size_t N, int nparts, int j, cu
 template <typename C>
 static void arnoldi_tail_multi(const Multi<C> &mm, int n, size_t N, int j, double tol, cudaStream_t st)
 {
-    k_scale_finish_m<C><<<dim3(vec_grid(N), n), kVT, 0, st>>>(mm, N, j, tol);
+    k_scale_finish_m<C><<<dim3(sweep_grid(N), n), kVT, 0, st>>>(mm, N, j, tol);
     g2_count_launches(1);
 }
 
