@@ -47,6 +47,28 @@ G2_D C twiddle_mul(C d, int e, const C *tw, int Lstride)
     return cmul(d, twid<C, INV>(tw, e * Lstride));
 }
 
+// Butterfly sum and difference.  Complex64 uses one packed add.rn.f32x2 / sub.rn.f32x2 (sm_100) each, which
+// round like two scalar adds: the register DFTs issue half the add instructions (the y passes are
+// issue-bound).
+G2_D double2 bf_add(double2 a, double2 b) { return a + b; }
+G2_D double2 bf_sub(double2 a, double2 b) { return a - b; }
+G2_D float2 bf_add(float2 a, float2 b)
+{
+    union U { float2 f; unsigned long long u; } ua, ub, uc;
+    ua.f = a;
+    ub.f = b;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(uc.u) : "l"(ua.u), "l"(ub.u));
+    return uc.f;
+}
+G2_D float2 bf_sub(float2 a, float2 b)
+{
+    union U { float2 f; unsigned long long u; } ua, ub, uc;
+    ua.f = a;
+    ub.f = b;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(uc.u) : "l"(ua.u), "l"(ub.u));
+    return uc.f;
+}
+
 // In-place N-point DFT of a[] (natural order in, bit-reversed order out).  L/N is the table stride.
 // If HALF_ZERO, a[N/2..N-1] are zero on entry (first stage pruned).
 template <typename C, int N, bool INV, bool HALF_ZERO>
@@ -64,8 +86,8 @@ G2_D void reg_dft_dif(C (&a)[N], const C *tw, int Lstride)
                     a[g + j + h] = twiddle_mul<C, N, INV>(u, j * (N / (2 * h)), tw, Lstride);
                 } else {
                     const C v = a[g + j + h];
-                    a[g + j] = u + v;
-                    a[g + j + h] = twiddle_mul<C, N, INV>(u - v, j * (N / (2 * h)), tw, Lstride);
+                    a[g + j] = bf_add(u, v);
+                    a[g + j + h] = twiddle_mul<C, N, INV>(bf_sub(u, v), j * (N / (2 * h)), tw, Lstride);
                 }
             }
         }
