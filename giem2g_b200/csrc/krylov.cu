@@ -566,22 +566,38 @@ __global__ void __launch_bounds__(kVT) k_scale_finish_m(Multi<C> mm, size_t N, i
     scale_finish_body<C>(mm.V[y] + (size_t)(j + 1) * N, mm.w[y], N, L, j, tol);
 }
 
-// ConstructCurrentSolution's triangular solve (gmres.F90:441-445): y = H(0:L,0:L)^-1 g
-__global__ void k_trisolve(Level L, const int *gate)
+// ConstructCurrentSolution's triangular solve (gmres.F90:441-445): y = H(0:L,0:L)^-1 g.  The block stages the
+// L x L triangle and g in shared memory with one coalesced load; thread 0 then substitutes in the same order
+// as the single-thread loop it replaces, so y is bit-for-bit the same (a chain of dependent L2 loads had made
+// this 13 us per call).  Launch with kTriThreads threads.
+constexpr int kTriThreads = 128;
+__global__ void __launch_bounds__(kTriThreads) k_trisolve(Level L, const int *gate)
 {
     if (gate && *gate == 0) return;
+    __shared__ double2 Hs[KMAX * (KMAX + 1)];  // column j < n of the triangle at j * KMAX, then g at n * KMAX
+    __shared__ double2 ys[KMAX];
     const int m = L.m, n = L.flags[F_L];
-    for (int i = n - 1; i >= 0; i--) {
-        double2 t = L.H[hix(i, m, m)];
-        for (int k = i + 1; k < n; k++) {
-            const double2 p = cmul_(L.H[hix(i, k, m)], L.y[k]);
-            t.x -= p.x;
-            t.y -= p.y;
-        }
-        const double2 d = L.H[hix(i, i, m)];
-        const double den = d.x * d.x + d.y * d.y;
-        L.y[i] = make_double2((t.x * d.x + t.y * d.y) / den, (t.y * d.x - t.x * d.y) / den);
+    for (int e = threadIdx.x; e < n * (n + 1); e += blockDim.x) {
+        const int i = e % n, j = e / n, col = j < n ? j : m;
+        Hs[i + j * KMAX] = L.H[hix(i, col, m)];
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double2 *g = Hs + n * KMAX;
+        for (int i = n - 1; i >= 0; i--) {
+            double2 t = g[i];
+            for (int k = i + 1; k < n; k++) {
+                const double2 p = cmul_(Hs[i + k * KMAX], ys[k]);
+                t.x -= p.x;
+                t.y -= p.y;
+            }
+            const double2 d = Hs[i + i * KMAX];
+            const double den = d.x * d.x + d.y * d.y;
+            ys[i] = make_double2((t.x * d.x + t.y * d.y) / den, (t.y * d.x - t.x * d.y) / den);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) L.y[i] = ys[i];
 }
 
 // start of a cycle: H(0,m) = beta, H(1..m, m) = 0, krylov active (gmres.F90:172-185)
@@ -1047,7 +1063,7 @@ static int inner_solve(IeOp *op, KrylovWork *k, const CI *v, const CI *x0, CI *x
         arnoldi_tail<CI>(k, L, Vi, j, wi, tol, krylov, st);
     }
     // FinalActions -> ConstructCurrentSolution (gmres.F90:423-458): x = x0 + V y
-    k_trisolve<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
+    k_trisolve<<<1, kTriThreads, 0, st>>>(L, solver); g2_count_launches(1);
     k_lincomb<CI, CI><<<g, kVT, 0, st>>>(x, 1.0, x, Vi, N, L.y, L.flags + F_L, N, solver); g2_count_launches(1);
     if (true_residual) {  // gmres.F90:402-419, result unused by the outer solver
         rc = apply_prec<CI>(op, x, ri, st, solver);
@@ -1225,7 +1241,7 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
         iter++;
         if (iter >= ctl.fgmres_maxit) break;
         // PrepareRestart: x += Z y; w = V g' (gmres.F90:333-379)
-        k_trisolve<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+        k_trisolve<<<1, kTriThreads, 0, st>>>(L, nullptr); g2_count_launches(1);
         k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, N, L.y, L.flags + F_L, N, nullptr); g2_count_launches(1);
         k_restart_g<<<1, 1, 0, st>>>(L); g2_count_launches(1);
         k_copy_g<<<1, 64, 0, st>>>(L); g2_count_launches(1);
@@ -1234,7 +1250,7 @@ static int outer_solve(IeOp *op, KrylovWork *k, const GIEM2G_FGMRES_CTL &ctl, GI
     }
     (void)L_used;
     // FinalActions (gmres.F90:382-421)
-    k_trisolve<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+    k_trisolve<<<1, kTriThreads, 0, st>>>(L, nullptr); g2_count_launches(1);
     k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, N, L.y, L.flags + F_L, N, nullptr); g2_count_launches(1);
     if ((rc = ie_apply_device64(op, k->x, k->r0, st))) return rc;
     k->applies64++;
@@ -1536,7 +1552,7 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         const int g = vec_grid(k->N);
         const int *solver = L.flags + F_SOLVER;
         CI *x = reinterpret_cast<CI *>(k->xin);
-        k_trisolve<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
+        k_trisolve<<<1, kTriThreads, 0, st>>>(L, solver); g2_count_launches(1);
         k_lincomb<CI, CI><<<g, kVT, 0, st>>>(x, 1.0, x, reinterpret_cast<const CI *>(k->Vi), k->N, L.y, L.flags + F_L,
                                              k->N, solver); g2_count_launches(1);
     }
@@ -1675,7 +1691,7 @@ static void batch_final_launch(BatchWork *b, int i, cudaStream_t st, int &rc)
     Level &L = k->Lo;
     const int g = vec_grid(k->N);
     CI *Z = reinterpret_cast<CI *>(k->Zo);
-    k_trisolve<<<1, 1, 0, st>>>(L, nullptr); g2_count_launches(1);
+    k_trisolve<<<1, kTriThreads, 0, st>>>(L, nullptr); g2_count_launches(1);
     k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, Z, k->N, L.y, L.flags + F_L, k->N, nullptr); g2_count_launches(1);
     if ((rc = ie_apply_device64(b->ops[i], k->x, k->r0, st))) return;
     k->applies64++;
@@ -1836,7 +1852,7 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
                 b->h_active[i] = 0;
                 continue;
             }
-            k_trisolve<<<1, 1, 0, st>>>(k->Lo, nullptr); g2_count_launches(1);
+            k_trisolve<<<1, kTriThreads, 0, st>>>(k->Lo, nullptr); g2_count_launches(1);
             k_lincomb<double2, CI><<<g, kVT, 0, st>>>(k->x, 1.0, k->x, reinterpret_cast<const CI *>(k->Zo), k->N,
                                                       k->Lo.y, k->Lo.flags + F_L, k->N, nullptr); g2_count_launches(1);
             k_restart_g<<<1, 1, 0, st>>>(k->Lo); g2_count_launches(1);
