@@ -186,20 +186,41 @@ G2_D void zrotg(double2 &ca, double2 cb, double &c, double2 &s)
 // end of Arnoldi step j (gmres.F90:283-326): H(j+1,j), rotations, Arnoldi misfit, exit test
 G2_D void arnoldi_finish_body(Level &L, int j, double tol)
 {
+    // run by every thread of one block: column j of H, the rotations so far and g(j), g(j+1) are staged in
+    // shared memory with one round of loads; thread 0 then applies the same operations in the same order
+    // as a single thread on global memory would (a chain of dependent L2 loads otherwise)
+    __shared__ double2 hc[KMAX + 1], sn_s[KMAX], gs[2];
+    __shared__ double cs_s[KMAX];
     const int m = L.m;
-    const double dnormw = L.scal[S_DNORMW];
-    L.H[hix(j + 1, j, m)] = make_double2(dnormw, 0.0);
-    for (int i = 0; i < j; i++) zrot1(L.H[hix(i, j, m)], L.H[hix(i + 1, j, m)], L.cs[i], L.sn[i]);
-    double2 h1 = L.H[hix(j, j, m)];
-    zrotg(h1, L.H[hix(j + 1, j, m)], L.cs[j], L.sn[j]);
-    zrot1(L.H[hix(j, m, m)], L.H[hix(j + 1, m, m)], L.cs[j], L.sn[j]);
-    zrot1(L.H[hix(j, j, m)], L.H[hix(j + 1, j, m)], L.cs[j], L.sn[j]);
-    L.H[hix(j + 1, j, m)] = make_double2(0.0, 0.0);
-    const double bea = cabs_(L.H[hix(j + 1, m, m)]) / L.scal[S_BN];
-    L.scal[S_BEA] = bea;
-    L.flags[F_ITER] += 1;
-    L.flags[F_L] = j + 1;
-    if (bea < tol || j + 1 >= m) L.flags[F_KRYLOV] = 0;
+    for (int i = threadIdx.x; i <= j + 1; i += blockDim.x) hc[i] = L.H[hix(i, j, m)];
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+        cs_s[i] = L.cs[i];
+        sn_s[i] = L.sn[i];
+    }
+    if (threadIdx.x < 2) gs[threadIdx.x] = L.H[hix(j + threadIdx.x, m, m)];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double dnormw = L.scal[S_DNORMW], bn = L.scal[S_BN];
+        hc[j + 1] = make_double2(dnormw, 0.0);
+        for (int i = 0; i < j; i++) zrot1(hc[i], hc[i + 1], cs_s[i], sn_s[i]);
+        double2 h1 = hc[j], sn;
+        double c;
+        zrotg(h1, hc[j + 1], c, sn);
+        zrot1(gs[0], gs[1], c, sn);
+        zrot1(hc[j], hc[j + 1], c, sn);
+        hc[j + 1] = make_double2(0.0, 0.0);
+        L.cs[j] = c;
+        L.sn[j] = sn;
+        L.H[hix(j, m, m)] = gs[0];
+        L.H[hix(j + 1, m, m)] = gs[1];
+        const double bea = cabs_(gs[1]) / bn;
+        L.scal[S_BEA] = bea;
+        L.flags[F_ITER] += 1;
+        L.flags[F_L] = j + 1;
+        if (bea < tol || j + 1 >= m) L.flags[F_KRYLOV] = 0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= j + 1; i += blockDim.x) L.H[hix(i, j, m)] = hc[i];
 }
 
 // ---- fused reductions: the last block to finish sums every block's partials ----------------------
@@ -547,7 +568,7 @@ G2_D void scale_finish_body(C *v, const C *w, size_t N, Level &L, int j, double 
     }
     for (i = Nw * E + t0; i < N; i += S) v[i] = scaled(w[i], inv);
     if (!last_block(L.counter)) return;
-    if (threadIdx.x == 0) arnoldi_finish_body(L, j, tol);
+    arnoldi_finish_body(L, j, tol);
 }
 template <typename C>
 __global__ void __launch_bounds__(kVT) k_scale_finish(C *v, const C *w, size_t N, Level L, int j, double tol,
