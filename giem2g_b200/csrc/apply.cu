@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_fy(con
     auto load = [&](int t, int yy) -> C { return col[yy * Z3 + t]; };
     auto store = [&](int t, int ky, C v) {
         int r, sy;
-        ky_to_slot(ky, Ny, r, sy);
+        ky_to_slot(ky, L / 2, r, sy);  // L = 2Ny: with the output index's range known, this folds per output
         dst[(r * 4 + sy) * Z3 + t] = v;
     };
     auto off = [&](int t, int n1, int k2) { return t + NL * (n1 + N1 * k2); };
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_by(con
     C *col = U1 + kx * Ny * Z3 + zc0;
     auto load = [&](int t, int ky) -> C {
         int r, sy;
-        ky_to_slot(ky, Ny, r, sy);
+        ky_to_slot(ky, L / 2, r, sy);  // L = 2Ny: folds per input at compile time
         return src[(r * 4 + sy) * Z3 + t];
     };
     auto store = [&](int t, int yy, C v) { col[yy * Z3 + t] = v; };
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(PassLB<R, CAP>::T, PassLB<R, CAP>::B) k_bx(con
     load_tw(tw, twg, L);
     __syncthreads();
     auto load = [&](int t, int kx) -> C {
-        return kx == Nx ? czero<C>() : U1[(kx * Ny + y) * ZL + zc0 + t];
+        return kx == L / 2 ? czero<C>() : U1[(kx * Ny + y) * ZL + zc0 + t];  // L = 2Nx
     };
     // a*x of each output, read before the inverse transform of its line (see fft4step_pre)
     auto pre = [&](int t, int x) -> C {

@@ -100,7 +100,8 @@ G2_D void reg_dft_dif(C (&a)[N], const C *tw, int Lstride)
 //   off(line, n1, k2) -> int        (shared-memory slot of the intermediate)
 // LF1/LF2: item ordering (true: line index fastest across threads; false: n1 / k2 fastest).  Items are
 // split with shifts and masks of the power-of-two line block; lines >= nl (a partial last block) are
-// skipped.
+// skipped.  n1 and k2 are masked to their ranges, which changes no value but lets the compiler resolve the
+// index arithmetic of the unrolled outputs (a slot mapping per output, for instance) at compile time.
 // The same transform run by a subset of the CTA's threads: thread tid of nthr, with sync() the barrier
 // of those threads (a named barrier when other warps of the CTA do other work).
 template <typename C, int N1, int N2, bool INV, bool PAD_IN, bool CROP_OUT, bool LF1, bool LF2, class LoadF,
@@ -113,7 +114,7 @@ G2_D void fft4step_part(C *sm, int nl, int lg_nl, const C *tw, LoadF load, Store
     const int n_items1 = (LF1 ? nlb : nl) * N1;
     for (int it = tid; it < n_items1; it += nthr) {
         int line, n1;
-        if (LF1) { line = it & (nlb - 1); n1 = it >> lg_nl; }
+        if (LF1) { line = it & (nlb - 1); n1 = (it >> lg_nl) & (N1 - 1); }
         else { n1 = it % N1; line = it / N1; }
         if (LF1 && line >= nl) continue;
         C a[N2];
@@ -134,7 +135,7 @@ G2_D void fft4step_part(C *sm, int nl, int lg_nl, const C *tw, LoadF load, Store
     const int n_items2 = (LF2 ? nlb : nl) * N2;
     for (int it = tid; it < n_items2; it += nthr) {
         int line, k2;
-        if (LF2) { line = it & (nlb - 1); k2 = it >> lg_nl; }
+        if (LF2) { line = it & (nlb - 1); k2 = (it >> lg_nl) & (N2 - 1); }
         else { k2 = it % N2; line = it / N2; }
         if (LF2 && line >= nl) continue;
         C a[N1];
@@ -162,7 +163,7 @@ G2_D void fft4step_part_ilp(C *sm, int nl, int lg_nl, const C *tw, LoadF load, S
 #pragma unroll
     for (int r = 0; r < IPT; r++) {
         const int it = tid + r * nthr;
-        const int line = it & (nlb - 1), n1 = it >> lg_nl;
+        const int line = it & (nlb - 1), n1 = (it >> lg_nl) & (N1 - 1);
         const bool ok = it < n_items1 && line < nl;
 #pragma unroll
         for (int n2 = 0; n2 < N2; n2++) a[r][n2] = (ok && n2 < NLD) ? load(line, n1 + N1 * n2) : czero<C>();
@@ -170,7 +171,7 @@ G2_D void fft4step_part_ilp(C *sm, int nl, int lg_nl, const C *tw, LoadF load, S
 #pragma unroll
     for (int r = 0; r < IPT; r++) {
         const int it = tid + r * nthr;
-        const int line = it & (nlb - 1), n1 = it >> lg_nl;
+        const int line = it & (nlb - 1), n1 = (it >> lg_nl) & (N1 - 1);
         if (it >= n_items1 || line >= nl) continue;
         reg_dft_dif<C, N2, INV, PAD_IN>(a[r], tw, L / N2);
 #pragma unroll
@@ -183,7 +184,7 @@ G2_D void fft4step_part_ilp(C *sm, int nl, int lg_nl, const C *tw, LoadF load, S
     sync();
     const int n_items2 = nlb * N2;
     for (int it = tid; it < n_items2; it += nthr) {
-        const int line = it & (nlb - 1), k2 = it >> lg_nl;
+        const int line = it & (nlb - 1), k2 = (it >> lg_nl) & (N2 - 1);
         if (line >= nl) continue;
         C b[N1];
 #pragma unroll
@@ -209,7 +210,7 @@ G2_D void fft4step_pre(C *sm, int nl, int lg_nl, const C *tw, LoadF load, PreF p
     const int n_items1 = (LF1 ? nlb : nl) * N1;
     for (int it = threadIdx.x; it < n_items1; it += blockDim.x) {
         int line, n1;
-        if (LF1) { line = it & (nlb - 1); n1 = it >> lg_nl; }
+        if (LF1) { line = it & (nlb - 1); n1 = (it >> lg_nl) & (N1 - 1); }
         else { n1 = it % N1; line = it / N1; }
         if (LF1 && line >= nl) continue;
         C a[N2];
@@ -230,7 +231,7 @@ G2_D void fft4step_pre(C *sm, int nl, int lg_nl, const C *tw, LoadF load, PreF p
     const int n_items2 = (LF2 ? nlb : nl) * N2;
     for (int it = threadIdx.x; it < n_items2; it += blockDim.x) {
         int line, k2;
-        if (LF2) { line = it & (nlb - 1); k2 = it >> lg_nl; }
+        if (LF2) { line = it & (nlb - 1); k2 = (it >> lg_nl) & (N2 - 1); }
         else { k2 = it % N2; line = it / N2; }
         if (LF2 && line >= nl) continue;
         decltype(pre(0, 0)) p[NOUT];
