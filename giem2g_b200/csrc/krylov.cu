@@ -952,10 +952,39 @@ static int krylov_alloc(IeOp *op, int mo, int mi, int precision)
 }
 
 // ---- launch helpers ------------------------------------------------------------------------------
+// Blocks per instance of a sweep: whole waves of the instantiation's resident blocks, as near as possible to
+// `want` (the instance's partial-sum slots, never more).  A grid that asks for 4 blocks per SM of a kernel
+// that fits 3 runs a last wave at a third of the bytes in flight: the FP64 first-dots sweep (80 registers)
+// streamed at 2.6 TB/s that way against 5 TB/s for the same data in the correction pass.
+static int sm_count()
+{
+    static const int sms = [] {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 1;
+    }();
+    return sms;
+}
+template <class F> static int resident_blocks(F fn)
+{
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kVT, 0) != cudaSuccess || b < 1) b = 1;
+    return b;
+}
+static int wave_grid(int per_sm, int want, int ninst)
+{
+    const int wave = per_sm * sm_count(), total = want * ninst;
+    int waves = (total + wave / 2) / wave;
+    if (waves < 1) waves = 1;
+    const int g = waves * wave / ninst;
+    return g < 1 ? 1 : (g < want ? g : want);
+}
 template <typename C, int K>
 static void launch_dots_first_k(KrylovWork *k, const C *V, const C *w, Level &L, const int *g, cudaStream_t st)
 {
-    k_dots_first_t<C, K><<<k->nparts, kVT, 0, st>>>(V, k->N, w, k->N, k->part, L, g);
+    static const int per_sm = resident_blocks(k_dots_first_t<C, K>);
+    k_dots_first_t<C, K><<<wave_grid(per_sm, k->nparts, 1), kVT, 0, st>>>(V, k->N, w, k->N, k->part, L, g);
 }
 template <typename C, int K>
 static void launch_pass_fused_k(KrylovWork *k, const C *V, C *w, Level &L, int p, const int *g, cudaStream_t st)
@@ -1016,7 +1045,8 @@ static void arnoldi_tail(KrylovWork *k, Level &L, C *V, int j, const C *w, doubl
 template <typename C, int K>
 static void launch_dots_first_km(const Multi<C> &mm, int n, size_t N, int nparts, cudaStream_t st)
 {
-    k_dots_first_m<C, K><<<dim3(nparts, n), kVT, 0, st>>>(mm, N, N);
+    static const int per_sm = resident_blocks(k_dots_first_m<C, K>);
+    k_dots_first_m<C, K><<<dim3(wave_grid(per_sm, nparts, n), n), kVT, 0, st>>>(mm, N, N);
 }
 template <typename C, int K>
 static void launch_pass_fused_km(const Multi<C> &mm, int n, size_t N, int nparts, int p, cudaStream_t st)
@@ -1814,8 +1844,36 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
                     k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
                     if ((r = ie_apply_device64(b->ops[i], k->tmp, k->w, st, go))) return r;
                 }
-                cgs<double2>(k, k->Lo, k->Vo, j, k->w, go, st);
-                arnoldi_tail<double2>(k, k->Lo, k->Vo, j, k->w, tol, go, st);
+            }
+            // the outer Arnoldi step of the active instances: runs of up to KMI with the same vector length share
+            // each launch (each keeps its own blocks, partials, gate and last-block step), as in the inner cycle
+            std::vector<int> act;
+            for (int i = 0; i < n; i++)
+                if (b->h_active[i]) act.push_back(i);
+            for (size_t c = 0; c < act.size();) {
+                KrylovWork *k0 = b->k[act[c]];
+                size_t e = c + 1;
+                while (e < act.size() && e - c < (size_t)KMI && b->k[act[e]]->N == k0->N &&
+                       b->k[act[e]]->nparts == k0->nparts)
+                    e++;
+                if (e - c == 1) {
+                    const int *go = k0->Lo.flags + F_KRYLOV;
+                    cgs<double2>(k0, k0->Lo, k0->Vo, j, k0->w, go, st);
+                    arnoldi_tail<double2>(k0, k0->Lo, k0->Vo, j, k0->w, tol, go, st);
+                } else {
+                    Multi<double2> mm{};
+                    for (size_t q = 0; q < e - c; q++) {
+                        KrylovWork *k = b->k[act[c + q]];
+                        mm.V[q] = k->Vo;
+                        mm.w[q] = k->w;
+                        mm.part[q] = k->part;
+                        mm.L[q] = k->Lo;
+                        mm.gate[q] = k->Lo.flags + F_KRYLOV;
+                    }
+                    cgs_multi<double2>(mm, (int)(e - c), k0->N, k0->nparts, j, st);
+                    arnoldi_tail_multi<double2>(mm, (int)(e - c), k0->N, j, tol, st);
+                }
+                c = e;
             }
             return G2_OK;
         };
