@@ -649,6 +649,40 @@ def run_apply_only(args):
     return 0
 
 
+def run_learned_only(args):
+    """The learned preconditioner's network (the committed weights) on one seeded input of the grid: `--reps`
+    inferences after `--warmup` untimed ones, CUDA events on torch's current stream (where the convolution
+    GEMMs run).  Reports ms per inference and the GEMM flops: per layer 2 x output voxels x Cout x K, with K
+    the stored (padded) 27 x Cin columns the tensor cores multiply."""
+    import torch
+    from giem2g_b200.learned import CIN, WEIGHTS, UNet3D, _kp
+
+    nz, ny, nx = args.nz, args.ny or args.nx, args.nx
+    net = UNet3D.from_file(WEIGHTS)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn(1, nz, ny, nx, CIN, device="cuda", generator=g)
+    level = {"in": 0, "e0": 0, "d1": 1, "e1": 1, "d2": 2, "e2": 2, "d3": 3, "b": 3, "u2": 2, "u1": 1, "u0": 0,
+             "out": 0}
+    flops = 0
+    for name, cin, cout, _ in UNet3D.LAYERS:
+        lv = level[name]
+        flops += 2 * (nz >> lv) * (ny >> lv) * (nx >> lv) * cout * _kp(cin)
+    with torch.no_grad():
+        for _ in range(args.warmup):
+            net(x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.reps):
+            net(x)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.reps
+    print(json.dumps({"mode": "learned-only", "grid": [nx, ny, nz], "reps": args.reps, "ms_per_inference": ms,
+                      "gemm_gflop_per_inference": flops / 1e9, "gemm_tflops_over_inference": flops / (ms * 1e-3) / 1e12}))
+    return 0
+
+
 def run_receivers_only(args):
     """Receiver fields at one grid (the workload the receiver profile captures): the receiver tensor of `--nr`
     receiver depths on the config_grf model (seed 7), its spectrum, and `--reps` recalculations of a seeded
@@ -756,9 +790,10 @@ def main():
     ap.add_argument("--variants", default=None,
                     help="pin the tile shapes instead of autotuning: v64,v32,vpair[,fft_lines[,fft_lines64]] "
                          "(for profilers)")
-    prof = ap.add_argument_group("profiler workloads (--apply-only, --receivers-only)")
+    prof = ap.add_argument_group("profiler workloads (--apply-only, --receivers-only, --learned-only)")
     prof.add_argument("--apply-only", action="store_true", help="a few IE applies at one grid")
     prof.add_argument("--receivers-only", action="store_true", help="receiver tensor and recalculations")
+    prof.add_argument("--learned-only", action="store_true", help="inferences of the learned preconditioner's net")
     prof.add_argument("--nx", type=int, default=128)
     prof.add_argument("--ny", type=int, default=None)
     prof.add_argument("--nz", type=int, default=32)
@@ -779,6 +814,8 @@ def main():
         if args.warmup == ap.get_default("warmup"):
             args.warmup = 1
         return run_receivers_only(args)
+    if args.learned_only:
+        return run_learned_only(args)
     rank, world, local = _env_int("RANK", 0), _env_int("WORLD_SIZE", 1), _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)
