@@ -1498,9 +1498,10 @@ int batch_history(void *h, int i, double *out, int max_len)
 // applies of the inner level: in_i -> out_i for every instance, paired where two instances share an
 // operator (complex64); flag selects the gate of the single applies (F_SOLVER or F_KRYLOV)
 template <typename CI, typename FIn, typename FOut>
-static int batch_apply(BatchWork *b, FIn in, FOut out, int flag, cudaStream_t st)
+static int batch_apply(BatchWork *b, FIn in, FOut out, int flag, cudaStream_t st, const BatchGroup *only = nullptr)
 {
     for (const BatchGroup &g : b->groups) {
+        if (only && &g != only) continue;
         const bool both = g.n == 2 && b->h_active[g.first] && b->h_active[g.first + 1];
         if (both && sizeof(CI) == sizeof(float2)) {
             float2 *U1 = nullptr, *Uh = nullptr;
@@ -1561,15 +1562,9 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         k_cycle_start<<<1, 1, 0, st>>>(L, solver); g2_count_launches(1);
         k_scale_by<CI><<<g, kVT, 0, st>>>(reinterpret_cast<CI *>(k->Vi), r, L.scal, S_BETA, k->N, solver); g2_count_launches(1);
     }
-    for (int j = 0; j < b->mi; j++) {
-        auto vj = [&](int i) { return reinterpret_cast<const CI *>(b->k[i]->Vi) + (size_t)j * b->k[i]->N; };
-        auto wi = [&](int i) { return reinterpret_cast<CI *>(b->k[i]->wi); };
-        if ((rc = batch_apply<CI>(b, vj, wi, F_KRYLOV, st))) return rc;
-        // Arnoldi step j of every active instance: runs of up to KMI instances with the same vector
-        // length share each launch (each instance keeps its own blocks, partials and gates)
-        std::vector<int> act;
-        for (int i = 0; i < n; i++)
-            if (b->h_active[i]) act.push_back(i);
+    // Arnoldi step j of the active instances in `act`: runs of up to KMI instances with the same vector length
+    // share each launch (each instance keeps its own blocks, partials and gates)
+    auto arnoldi_step = [&](const std::vector<int> &act, int j) {
         for (size_t c = 0; c < act.size();) {
             KrylovWork *k0 = b->k[act[c]];
             size_t e = c + 1;
@@ -1594,6 +1589,22 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
                 arnoldi_tail_multi<CI>(mm, (int)(e - c), k0->N, j, tol, st);
             }
             c = e;
+        }
+    };
+    // Each operator group (one frequency's polarisations) runs its apply and then its Arnoldi step before the
+    // next group's apply, so the group's fresh w is still in L2 when its Gram-Schmidt reads it (with all
+    // applies first, a 16-instance sweep re-read every w from DRAM).  Per instance the sequence of kernels is
+    // unchanged.
+    for (int j = 0; j < b->mi; j++) {
+        auto vj = [&](int i) { return reinterpret_cast<const CI *>(b->k[i]->Vi) + (size_t)j * b->k[i]->N; };
+        auto wi = [&](int i) { return reinterpret_cast<CI *>(b->k[i]->wi); };
+        for (const BatchGroup &g : b->groups) {
+            std::vector<int> act;
+            for (int i = g.first; i < g.first + g.n; i++)
+                if (b->h_active[i]) act.push_back(i);
+            if (act.empty()) continue;
+            if ((rc = batch_apply<CI>(b, vj, wi, F_KRYLOV, st, &g))) return rc;
+            arnoldi_step(act, j);
         }
     }
     for (int i = 0; i < n; i++) {
@@ -1831,49 +1842,51 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
             }
             int r = batch_inner_fixed<CI>(b, tol, st);
             if (r) return r;
-            for (int i = 0; i < n; i++) {
-                if (!b->h_active[i]) continue;
-                KrylovWork *k = b->k[i];
-                const int g = vec_grid(k->N);
-                const int *go = k->Lo.flags + F_KRYLOV;
-                CI *Zj = reinterpret_cast<CI *>(k->Zo) + (size_t)j * k->N;
-                k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
-                if (sizeof(CI) == sizeof(double2)) {
-                    if ((r = ie_apply_device64(b->ops[i], reinterpret_cast<const double2 *>(Zj), k->w, st, go))) return r;
-                } else {
-                    k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
-                    if ((r = ie_apply_device64(b->ops[i], k->tmp, k->w, st, go))) return r;
+            // per operator group: the FP64 applies, then the group's outer Arnoldi step (w still in L2), with
+            // the group's instances sharing each CGS and scaling launch
+            for (const BatchGroup &gr : b->groups) {
+                std::vector<int> act;
+                for (int i = gr.first; i < gr.first + gr.n; i++) {
+                    if (!b->h_active[i]) continue;
+                    act.push_back(i);
+                    KrylovWork *k = b->k[i];
+                    const int g = vec_grid(k->N);
+                    const int *go = k->Lo.flags + F_KRYLOV;
+                    CI *Zj = reinterpret_cast<CI *>(k->Zo) + (size_t)j * k->N;
+                    k_axpby<CI, CI, CI><<<g, kVT, 0, st>>>(Zj, 1.0, reinterpret_cast<const CI *>(k->xin), 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
+                    if (sizeof(CI) == sizeof(double2)) {
+                        if ((r = ie_apply_device64(b->ops[i], reinterpret_cast<const double2 *>(Zj), k->w, st, go))) return r;
+                    } else {
+                        k_axpby<double2, CI, CI><<<g, kVT, 0, st>>>(k->tmp, 1.0, Zj, 0.0, (const CI *)nullptr, k->N, go); g2_count_launches(1);
+                        if ((r = ie_apply_device64(b->ops[i], k->tmp, k->w, st, go))) return r;
+                    }
                 }
-            }
-            // the outer Arnoldi step of the active instances: runs of up to KMI with the same vector length share
-            // each launch (each keeps its own blocks, partials, gate and last-block step), as in the inner cycle
-            std::vector<int> act;
-            for (int i = 0; i < n; i++)
-                if (b->h_active[i]) act.push_back(i);
-            for (size_t c = 0; c < act.size();) {
-                KrylovWork *k0 = b->k[act[c]];
-                size_t e = c + 1;
-                while (e < act.size() && e - c < (size_t)KMI && b->k[act[e]]->N == k0->N &&
-                       b->k[act[e]]->nparts == k0->nparts)
-                    e++;
-                if (e - c == 1) {
+                if (act.size() == 1) {
+                    KrylovWork *k0 = b->k[act[0]];
                     const int *go = k0->Lo.flags + F_KRYLOV;
                     cgs<double2>(k0, k0->Lo, k0->Vo, j, k0->w, go, st);
                     arnoldi_tail<double2>(k0, k0->Lo, k0->Vo, j, k0->w, tol, go, st);
-                } else {
+                } else if (act.size() == 2 && b->k[act[0]]->N == b->k[act[1]]->N &&
+                           b->k[act[0]]->nparts == b->k[act[1]]->nparts) {
                     Multi<double2> mm{};
-                    for (size_t q = 0; q < e - c; q++) {
-                        KrylovWork *k = b->k[act[c + q]];
+                    for (size_t q = 0; q < act.size(); q++) {
+                        KrylovWork *k = b->k[act[q]];
                         mm.V[q] = k->Vo;
                         mm.w[q] = k->w;
                         mm.part[q] = k->part;
                         mm.L[q] = k->Lo;
                         mm.gate[q] = k->Lo.flags + F_KRYLOV;
                     }
-                    cgs_multi<double2>(mm, (int)(e - c), k0->N, k0->nparts, j, st);
-                    arnoldi_tail_multi<double2>(mm, (int)(e - c), k0->N, j, tol, st);
+                    cgs_multi<double2>(mm, 2, b->k[act[0]]->N, b->k[act[0]]->nparts, j, st);
+                    arnoldi_tail_multi<double2>(mm, 2, b->k[act[0]]->N, j, tol, st);
+                } else {
+                    for (int i : act) {
+                        KrylovWork *k = b->k[i];
+                        const int *go = k->Lo.flags + F_KRYLOV;
+                        cgs<double2>(k, k->Lo, k->Vo, j, k->w, go, st);
+                        arnoldi_tail<double2>(k, k->Lo, k->Vo, j, k->w, tol, go, st);
+                    }
                 }
-                c = e;
             }
             return G2_OK;
         };
