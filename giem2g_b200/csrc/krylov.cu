@@ -1385,11 +1385,12 @@ int krylov_history(IeOp *op, double *out, int max_len)
 namespace {
 
 // outer_go: the instance's outer Krylov flag (F_KRYLOV of its outer level); an inner cycle enqueued after the
-// instance converged (one outer step ahead of the host, see batch_outer) does nothing
-__global__ void k_set_bn_masked(Level L, const int *active, const int *outer_go)
+// instance converged (one outer step ahead of the host, see batch_outer) does nothing.  (Masked instances
+// launch nothing: each mask has its own captured cycle.)
+__global__ void k_set_bn_masked(Level L, const int *outer_go)
 {
     L.scal[S_BN] = sqrt(L.scal[S_NRM2]);
-    L.flags[F_SOLVER] = (L.scal[S_BN] < ZERO_THRESHOLD || *active == 0 || *outer_go == 0) ? 0 : 1;
+    L.flags[F_SOLVER] = (L.scal[S_BN] < ZERO_THRESHOLD || *outer_go == 0) ? 0 : 1;
     L.flags[F_ITER] = 0;
     L.flags[F_KRYLOV] = L.flags[F_SOLVER];
     L.flags[F_L] = 0;
@@ -1408,8 +1409,7 @@ struct BatchWork {
     std::vector<IeOp *> ops;
     std::vector<KrylovWork *> k;
     std::vector<BatchGroup> groups;
-    int *d_active = nullptr;
-    std::vector<int> h_active, dev_active;  // host mask and its copy on the device
+    std::vector<int> h_active;  // instances still running (each mask has its own captured inner cycle)
     double2 *d_stage = nullptr;  // host-array solves: E_bkg[n] then E_sol[n] (complex128)
     // pinned host copies of the outer levels' scalars and flags, two slots (outer step j uses slot j % 2),
     // each completed by its own event
@@ -1440,7 +1440,6 @@ static void batch_destroy(BatchWork *b)
     if (b->h_pin) cudaFreeHost(b->h_pin);
     for (cudaEvent_t e : b->ev_pull)
         if (e) cudaEventDestroy(e);
-    if (b->d_active) cudaFree(b->d_active);
     if (b->d_stage) cudaFree(b->d_stage);
     delete b;
 }
@@ -1476,9 +1475,7 @@ int batch_create(IeOp *const *ops, int n, int mo, int mi, int precision, void **
         b->groups.push_back(g);
         i += g.n;
     }
-    if (cudaMalloc(&b->d_active, sizeof(int) * n) != cudaSuccess) { batch_destroy(b); return G2_ERR_NOMEM; }
     b->h_active.assign(n, 1);
-    b->dev_active.assign(n, -1);
     b->history.resize(n);
     *out = b;
     return G2_OK;
@@ -1540,8 +1537,8 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
         Level &L = k->Li;
         const int g = vec_grid(k->N);
         k_zero_level<<<1, 256, 0, st>>>(L); g2_count_launches(1);
-        norm2<CI>(k, reinterpret_cast<const CI *>(k->vin), L.scal + S_NRM2, b->d_active + i, st);
-        k_set_bn_masked<<<1, 1, 0, st>>>(L, b->d_active + i, k->Lo.flags + F_KRYLOV); g2_count_launches(1);
+        norm2<CI>(k, reinterpret_cast<const CI *>(k->vin), L.scal + S_NRM2, nullptr, st);
+        k_set_bn_masked<<<1, 1, 0, st>>>(L, k->Lo.flags + F_KRYLOV); g2_count_launches(1);
         k_copy_or_zero<CI><<<g, kVT, 0, st>>>(reinterpret_cast<CI *>(k->xin), reinterpret_cast<const CI *>(k->vin),
                                              L.scal, k->N); g2_count_launches(1);
     }
@@ -1625,10 +1622,6 @@ static int batch_inner(BatchWork *b, double tol, cudaStream_t st)
 template <typename CI>
 static int batch_inner_fixed(BatchWork *b, double tol, cudaStream_t st)
 {
-    if (b->h_active != b->dev_active) {
-        G2_CUDA_CHECK(cudaMemcpyAsync(b->d_active, b->h_active.data(), sizeof(int) * b->n, cudaMemcpyHostToDevice, st));
-        b->dev_active = b->h_active;
-    }
     std::vector<long long> cv;
     for (IeOp *op : b->ops) cv.push_back(op->config_gen);
     const char *ng = std::getenv("GIEM2G_NO_GRAPHS");
@@ -1704,45 +1697,59 @@ struct BatchScal {
     double s[S_NSCAL];
     int f[F_NFLAGS];
 };
-static int batch_pull(BatchWork *b, std::vector<BatchScal> &h, cudaStream_t st)
-{
-    for (int i = 0; i < b->n; i++) {
-        if (!b->h_active[i]) continue;
-        G2_CUDA_CHECK(cudaMemcpyAsync(h[i].s, b->k[i]->Lo.scal, sizeof(h[i].s), cudaMemcpyDeviceToHost, st));
-        G2_CUDA_CHECK(cudaMemcpyAsync(h[i].f, b->k[i]->Lo.flags, sizeof(h[i].f), cudaMemcpyDeviceToHost, st));
-    }
-    G2_CUDA_CHECK(cudaStreamSynchronize(st));
-    for (IeOp *op : b->ops) {
-        const int rc = ie_check_device_error(op);
-        if (rc) return rc;
-    }
-    return G2_OK;
-}
-
-// The same copies into pinned slot `slot`, completed by an event instead of a synchronisation, so the host can
-// enqueue more work before it waits (batch_outer's outer step j + 1).
-static int batch_pull_async(BatchWork *b, int slot, cudaStream_t st)
+// Copies of the outer level's scalars and flags of instances `which` into pinned slot `slot` (pageable
+// destinations made every such read a staged, blocking copy), completed by the slot's event.
+static int batch_pull_start(BatchWork *b, const std::vector<int> &which, int slot, cudaStream_t st)
 {
     if (!b->h_pin) {
         G2_CUDA_CHECK(cudaMallocHost(&b->h_pin, 2 * sizeof(BatchScal) * b->n));
         for (cudaEvent_t &e : b->ev_pull) G2_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     BatchScal *h = reinterpret_cast<BatchScal *>(b->h_pin) + (size_t)slot * b->n;
-    for (int i = 0; i < b->n; i++) {
-        if (!b->h_active[i]) continue;
+    for (int i : which) {
         G2_CUDA_CHECK(cudaMemcpyAsync(h[i].s, b->k[i]->Lo.scal, sizeof(h[i].s), cudaMemcpyDeviceToHost, st));
         G2_CUDA_CHECK(cudaMemcpyAsync(h[i].f, b->k[i]->Lo.flags, sizeof(h[i].f), cudaMemcpyDeviceToHost, st));
     }
     G2_CUDA_CHECK(cudaEventRecord(b->ev_pull[slot], st));
     return G2_OK;
 }
-static int batch_pull_wait(BatchWork *b, int slot, std::vector<BatchScal> &h)
+static int batch_pull_finish(BatchWork *b, const std::vector<int> &which, int slot, std::vector<BatchScal> &h)
 {
     G2_CUDA_CHECK(cudaEventSynchronize(b->ev_pull[slot]));
     const BatchScal *p = reinterpret_cast<const BatchScal *>(b->h_pin) + (size_t)slot * b->n;
-    for (int i = 0; i < b->n; i++)
-        if (b->h_active[i]) h[i] = p[i];
+    for (int i : which) h[i] = p[i];
     return G2_OK;
+}
+static std::vector<int> active_list(const BatchWork *b)
+{
+    std::vector<int> a;
+    for (int i = 0; i < b->n; i++)
+        if (b->h_active[i]) a.push_back(i);
+    return a;
+}
+// per-instance host copies of the active instances' scalars and flags, one synchronisation for all
+static int batch_pull(BatchWork *b, std::vector<BatchScal> &h, cudaStream_t st)
+{
+    const std::vector<int> act = active_list(b);
+    int rc = batch_pull_start(b, act, 0, st);
+    if (!rc) rc = batch_pull_finish(b, act, 0, h);
+    if (rc) return rc;
+    for (IeOp *op : b->ops) {
+        const int e = ie_check_device_error(op);
+        if (e) return e;
+    }
+    return G2_OK;
+}
+
+// The same copies into pinned slot `slot` without waiting, so the host can enqueue more work before it waits
+// (batch_outer's outer step j + 1).
+static int batch_pull_async(BatchWork *b, int slot, cudaStream_t st)
+{
+    return batch_pull_start(b, active_list(b), slot, st);
+}
+static int batch_pull_wait(BatchWork *b, int slot, std::vector<BatchScal> &h)
+{
+    return batch_pull_finish(b, active_list(b), slot, h);
 }
 
 // FinalActions of instance i (gmres.F90:382-421) after the host learned that it stops
@@ -1962,10 +1969,10 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
         for (int i = 0; i < n; i++) any_fin = any_fin || finishing[i];
         if (any_fin) {
             // read the true residuals of the instances that finished (pull reads active ones only)
+            std::vector<int> fin;
             for (int i = 0; i < n; i++)
-                if (finishing[i])
-                    G2_CUDA_CHECK(cudaMemcpyAsync(h[i].s, b->k[i]->Lo.scal, sizeof(h[i].s), cudaMemcpyDeviceToHost, st));
-            G2_CUDA_CHECK(cudaStreamSynchronize(st));
+                if (finishing[i]) fin.push_back(i);
+            if ((rc = batch_pull_start(b, fin, 0, st)) || (rc = batch_pull_finish(b, fin, 0, h))) return rc;
             for (int i = 0; i < n; i++) {
                 if (!finishing[i]) continue;
                 const double be = std::sqrt(h[i].s[S_NRM2]) / bn[i];
