@@ -195,3 +195,40 @@ def test_eight_instance_sweep_batch(g2lib, orc):
     assert np.linalg.norm(r) / np.linalg.norm(rhs) < 1.5e-8
     for _, op in ops:
         op.delete()
+
+
+@pytest.mark.parametrize("max_restart", [50, 2])
+def test_batched_restarts_match_single(g2lib, max_restart):
+    """Outer basis 3 and inner basis 2 force restart cycles (the host runs one outer step ahead inside a cycle
+    and stops at its end); with max_restart = 2 the instances stop unconverged (status -1).  In FP64 every
+    batched instance reproduces its single solve: status, iterations, misfit history and solution."""
+    import torch
+    ops, inst = _two_frequency_setup(g2lib)
+    d_e = [torch.from_numpy(np.ascontiguousarray(e).ravel()).to("cuda") for _, e in inst]
+    kw = dict(outer_buf=3, inner_buf=2, max_restart=max_restart)
+    tol = 1e-10
+    single = []
+    for (op, _), x in zip(inst, d_e):
+        y = torch.empty_like(x)
+        single.append((op.solve_device(x.data_ptr(), y.data_ptr(), None, tol=tol, precision=0, **kw), y))
+    b = g2lib.Batch([op for op, _ in inst], precision=0, **kw)
+    d_s = [torch.empty_like(x) for x in d_e]
+    infos = b.solve_device([x.data_ptr() for x in d_e], [y.data_ptr() for y in d_s], tol=tol)
+    torch.cuda.synchronize()
+    for i, (info1, y1) in enumerate(single):
+        assert infos[i].stat == info1.stat
+        assert infos[i].iterations == info1.iterations
+        assert np.allclose(infos[i].misfits, info1.misfits, rtol=1e-10, atol=0)
+        assert rel(d_s[i].cpu().numpy(), y1.cpu().numpy()) < 1e-12
+        if max_restart == 2:
+            assert infos[i].iterations <= 6                      # two cycles of three outer steps at most
+            assert infos[i].stat == 1 or infos[i].iterations == 6
+        else:
+            assert infos[i].stat == 1
+    if max_restart == 50:
+        assert max(i.iterations for i in infos) > 3              # the batch went through a restart
+    else:
+        assert any(i.stat == -1 for i in infos)                   # and one instance stopped unconverged
+    b.delete()
+    for op in ops:
+        op.delete()
