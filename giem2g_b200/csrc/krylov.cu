@@ -1786,12 +1786,20 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
         info[i].be = -1.0;
         info[i].stat = -1;
     }
-    // gmres.F90:129-168 for every instance
+    // gmres.F90:129-168 for every instance, with one host read: the initial residual is gated on the device
+    // flag k_set_bn clears for a zero right-hand side, so the host need not read ||b|| before launching it
     for (int i = 0; i < n; i++) {
         KrylovWork *k = b->k[i];
+        const int g = vec_grid(k->N);
+        const int *solver = k->Lo.flags + F_SOLVER;
         k_zero_level<<<1, 256, 0, st>>>(k->Lo); g2_count_launches(1);
         norm2<double2>(k, k->b, k->Lo.scal + S_NRM2, nullptr, st);
         k_set_bn<<<1, 1, 0, st>>>(k->Lo); g2_count_launches(1);
+        if ((rc = ie_apply_device64(b->ops[i], k->x, k->r0, st, solver))) return rc;
+        k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, k->N, solver); g2_count_launches(1);
+        k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->w, 1.0, k->r0, 0.0, (const double2 *)nullptr, k->N, solver); g2_count_launches(1);
+        norm2<double2>(k, k->w, k->Lo.scal + S_NRM2, solver, st);
+        k_set_beta<<<1, 1, 0, st>>>(k->Lo, tol); g2_count_launches(1);
     }
     if ((rc = batch_pull(b, h, st))) return rc;
     for (int i = 0; i < n; i++) {
@@ -1803,15 +1811,8 @@ static int batch_outer(BatchWork *b, const GIEM2G_FGMRES_CTL &ctl, GIEM2G_RESULT
             b->h_active[i] = 0;
             continue;
         }
-        const int g = vec_grid(k->N);
-        if ((rc = ie_apply_device64(b->ops[i], k->x, k->r0, st))) return rc;
         k->applies64++;
-        k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->r0, 1.0, k->b, -1.0, k->r0, k->N, nullptr); g2_count_launches(1);
-        k_axpby<double2, double2, double2><<<g, kVT, 0, st>>>(k->w, 1.0, k->r0, 0.0, (const double2 *)nullptr, k->N, nullptr); g2_count_launches(1);
-        norm2<double2>(k, k->w, k->Lo.scal + S_NRM2, nullptr, st);
-        k_set_beta<<<1, 1, 0, st>>>(k->Lo, tol); g2_count_launches(1);
     }
-    if ((rc = batch_pull(b, h, st))) return rc;
     for (int i = 0; i < n; i++) {
         if (!b->h_active[i]) continue;
         if (h[i].s[S_BETA] / bn[i] < tol) {
