@@ -519,8 +519,34 @@ __global__ void __launch_bounds__(kVT) k_norm2_fused(const C *__restrict__ w, si
 {
     if (gate && *gate == 0) return;
     using R = typename RealOf<C>::T;
+    using W = typename Wide<C>::T;
+    constexpr int E = Wide<C>::E, U = 4;  // 16-byte words, U of them loaded before the first product
     R ax[1] = {R(0)}, ay[1] = {R(0)};
-    for (size_t i = blockIdx.x * (size_t)kVT + threadIdx.x; i < N; i += (size_t)gridDim.x * kVT) {
+    const size_t S = (size_t)gridDim.x * kVT, t0 = blockIdx.x * (size_t)kVT + threadIdx.x;
+    const size_t Nw = wide_words<C>(N, N);
+    const W *__restrict__ ww = reinterpret_cast<const W *>(w);
+    size_t i = t0;
+    for (; i + (U - 1) * S < Nw; i += U * S) {
+        W v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = ww[i + u * S];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const C a = part_of(v[u], e);
+                ax[0] += a.x * a.x + a.y * a.y;
+            }
+    }
+    for (; i < Nw; i += S) {
+        const W v = ww[i];
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const C a = part_of(v, e);
+            ax[0] += a.x * a.x + a.y * a.y;
+        }
+    }
+    for (i = Nw * E + t0; i < N; i += S) {
         const C wv = w[i];
         ax[0] += wv.x * wv.x + wv.y * wv.y;
     }
