@@ -4,8 +4,10 @@ The contraction kernel has several compile-time tile shapes (j-slices per unit, 
 pipeline depth) per precision and Nz (giem2g_contract_variants; precision 2 is the paired complex64
 apply of two vectors).  The best one depends on Nz, the
 precision and the grid, so the tuner times every variant with CUDA events on the operator's own
-buffers (a few full applies each) and keeps the fastest in the operator; results are cached per
-(Nx, Ny, Nz, precision) in a JSON file next to this module when one is given.
+buffers and keeps the fastest in the operator; results are cached per (Nx, Ny, Nz, precision) in a JSON
+file next to this module when one is given.  Each candidate is timed in `rounds` rounds of `reps` full
+applies and scored by its fastest round, so a transient slowdown (another process, a clock dip) during
+one round does not decide the pick.
 """
 from __future__ import annotations
 
@@ -13,7 +15,26 @@ import json
 import os
 
 
-def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> dict:
+def _time_rounds(run, stream, reps: int, rounds: int) -> float:
+    """Fastest of `rounds` CUDA-event timings of `reps` calls of run() (ms per call), after 2 warm-up calls."""
+    import torch
+    for _ in range(2):
+        run()
+    best = None
+    for _ in range(rounds):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        best = ms if best is None else min(best, ms)
+    return best
+
+
+def autotune_contraction(op, reps: int = 5, cache_path: str | None = None, rounds: int = 3) -> dict:
     import torch
 
     key = f"{op.Nx}x{op.Ny}x{op.Nz}"
@@ -49,16 +70,7 @@ def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> di
         best, all_ms = None, []
         for v in range(nv):
             op.set_contract_variant(prec, v)
-            for _ in range(2):
-                run()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e0.record(stream)
-            for _ in range(reps):
-                run()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
+            ms = _time_rounds(run, stream, reps, rounds)
             all_ms.append(round(ms, 5))
             if best is None or ms < best[1]:
                 best = (v, ms)
@@ -71,16 +83,7 @@ def autotune_contraction(op, reps: int = 5, cache_path: str | None = None) -> di
         best, all_ms = None, []
         for lines in (32, 16, 8):
             op.set_fft_lines(lines, precision=prec)
-            for _ in range(2):
-                run()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e0.record(stream)
-            for _ in range(reps):
-                run()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
+            ms = _time_rounds(run, stream, reps, rounds)
             all_ms.append(round(ms, 5))
             if best is None or ms < best[1]:
                 best = (lines, ms)
