@@ -294,7 +294,8 @@ struct CfgL {
 
 // PK (complex64): the packed 3-multiply form of k_contract_tma, two instructions per complex multiply-add.
 // VS: the NP vectors of a unit split over VS lane groups (LanePts): fewer points and registers per lane.
-template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4, bool PK, int VS = 1>
+// UR: j iterations of the unit sums unrolled together (wl_unit_sums)
+template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP, int MINB, bool M4, bool PK, int VS = 1, int UR = 2>
 __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB, VS>::NTHREADS, MINB)
     k_contract_wl(const typename V2<R>::T *__restrict__ G, typename V2<R>::T *__restrict__ Uhat, int Ny,
                   long long nunits, int *err, const int *gate)
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB, VS>::NTH
         const C2 *gb = reinterpret_cast<const C2 *>(st);
         const C2 *ub = reinterpret_cast<const C2 *>(st + Cfg::TBYTES);  // [pt][c][j]
         R v[Cfg::NR];
-        wl_unit_sums<R, NZ, SL, NP, M4, PK, VS>(gb, ub, z, s, v, vv);
+        wl_unit_sums<R, NZ, SL, NP, M4, PK, VS, UR>(gb, ub, z, s, v, vv);
         mbar_arrive(&empty[slot]);  // this lane's reads of the stage are done
 
         const long long unit = first + it * stride;
@@ -649,11 +650,11 @@ int launch_cfg(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cud
 }
 
 template <typename R, int NZ, int SL, int NG, int NSTAGE, int NP = 1, int MINB = 1, bool M4 = false, bool PK = false,
-          int VS = 1>
+          int VS = 1, int UR = 2>
 int launch_wl(const void *G, void *Uhat, int Nx, int Ny, int *err, int nsm, cudaStream_t st, const int *gate)
 {
     using Cfg = CfgL<R, NZ, SL, NG, NSTAGE, NP, MINB, VS>;
-    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4, PK, VS>;
+    auto kern = k_contract_wl<R, NZ, SL, NG, NSTAGE, NP, MINB, M4, PK, VS, UR>;
     nsm *= MINB;
     static bool attr = false;
     if (!attr) {
@@ -685,8 +686,8 @@ int sm_count()
 // on the operator's own buffers and stores its pick in the operator.
 int ie_contract_variants(int precision, int Nz)
 {
-    if (precision == 0) return Nz == 32 ? 11 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
-    return Nz == 32 ? 24 : (Nz == 8 || Nz == 16 || Nz == 48 ? 4 : 0);
+    if (precision == 0) return Nz == 32 ? 12 : (Nz == 8 || Nz == 16 || Nz == 48 ? 2 : 0);
+    return Nz == 32 ? 25 : (Nz == 8 || Nz == 16 || Nz == 48 ? 4 : 0);
 }
 
 // Returns G2_ERR_UNSUPPORTED when no specialised configuration exists (caller uses the generic kernel).
@@ -715,6 +716,7 @@ int ie_contract_fast64(const double2 *G, double2 *Uhat, int Nx, int Ny, int Nz, 
         if (v == 8) return launch_wl<double, 32, 2, 3, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 9) return launch_wl<double, 32, 2, 4, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 10) return launch_wl<double, 32, 4, 2, 3, 1, 1, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        if (v == 11) return launch_wl<double, 32, 4, 2, 3, 1, 1, false, false, 1, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<double, 32, 8, 1, 3>(G, Uhat, Nx, Ny, err, n, st, gate);
     default: return G2_ERR_UNSUPPORTED;
     }
@@ -760,6 +762,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         case 21: return launch_wl<float, 32, 2, 6, 6, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 22: return launch_wl<float, 32, 2, 4, 6, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
         case 23: return launch_wl<float, 32, 4, 4, 6, 1, 1, false, true>(G, Uhat, Nx, Ny, err, n, st, gate);
+        case 24: return launch_wl<float, 32, 2, 6, 6, 1, 1, false, true, 1, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
         default: return launch_cfg<float, 32, 8, 1, 5>(G, Uhat, Nx, Ny, err, n, st, gate);
         }
     case 48:
@@ -775,7 +778,7 @@ int ie_contract_fast32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
 // The spectrum holds [unit][slot][vector][3Nz].  Variants: 0 the direct kernel with the two vectors spread
 // over threads, 1 the direct kernel with both vectors in each thread's registers, 2 (and 3) the
 // Walsh-basis packed kernel.
-int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 20 : (Nz == 48 ? 6 : ((Nz == 8 || Nz == 16) ? 4 : 0)); }
+int ie_contract_pair_variants(int Nz) { return Nz == 32 ? 21 : (Nz == 48 ? 6 : ((Nz == 8 || Nz == 16) ? 4 : 0)); }
 int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, int *err, cudaStream_t st,
                        const int *gate, int v)
 {
@@ -812,6 +815,8 @@ int ie_contract_pair32(const float2 *G, float2 *Uhat, int Nx, int Ny, int Nz, in
         if (v == 17) return launch_wl<float, 32, 2, 4, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 18) return launch_wl<float, 32, 2, 2, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
         if (v == 19) return launch_wl<float, 32, 4, 2, 5, 2, 1, false, true, 2>(G, Uhat, Nx, Ny, err, n, st, gate);
+        // variant 14 with four j iterations unrolled together
+        if (v == 20) return launch_wl<float, 32, 2, 4, 5, 2, 1, false, true, 1, 4>(G, Uhat, Nx, Ny, err, n, st, gate);
         return launch_cfg<float, 32, 4, 2, 2, 2, true>(G, Uhat, Nx, Ny, err, n, st, gate);
     case 48:
         if (v == 1) return launch_cfg<float, 48, 4, 1, 2, 2>(G, Uhat, Nx, Ny, err, n, st, gate);

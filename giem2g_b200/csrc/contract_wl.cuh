@@ -76,7 +76,9 @@ template <int NP, int VS> struct LanePts {
     static G2_HD int gp(int p, int vv) { return (p / NPL) * NP + vv * NPL + p % NPL; }
 };
 
-template <typename R, int NZ, int SL, int NP, bool M4, bool PK, int VS = 1>
+// UR: j iterations unrolled together (4 let the paired complex64 tile overlap more shared-memory loads with its
+// FMAs: 192.6 against 199.3 us at 128x128x32, at 167 instead of 157 registers)
+template <typename R, int NZ, int SL, int NP, bool M4, bool PK, int VS = 1, int UR = 2>
 G2_D void wl_unit_sums(const typename V2<R>::T *__restrict__ gb, const typename V2<R>::T *__restrict__ ub, int z,
                        int s, R (&v)[2 * 3 * LanePts<NP, VS>::PL], int vv = 0)
 {
@@ -98,7 +100,7 @@ G2_D void wl_unit_sums(const typename V2<R>::T *__restrict__ gb, const typename 
         }
     const C2 *gxx = gb, *gxy = gb + P, *gyy = gb + 2 * P, *gzz = gb + 3 * P;
     const C2 *gxz = gb + 4 * P, *gyz = gb + 4 * P + NZ * NZ;
-#pragma unroll 2
+#pragma unroll UR
     for (int jj = 0; jj < JS; jj++) {
         const int j = jj * SL + s;
         const int si = sym_idx<NZ>(z, j);
