@@ -28,13 +28,14 @@ constexpr int kThreads = 256;
 
 // Launch bounds of the FFT passes.  CAP = 0: any block up to 256 threads, registers as the compiler likes
 // (100-130 in FP64, 90-100 in complex64 at 2Ny = 256).  CAP = 1 holds more blocks per SM -- the passes are
-// latency-bound at 14-16 resident warps: complex64 at 64 registers (4 blocks of 256 threads), FP64 at 96
-// (5 blocks of 128 threads, so only for 8 lines per CTA).  Measured per apply at 128x128x32: complex64 passes
-// 88 -> 77 us, FP64 139 -> 128 us; tighter caps spill and lose.  Used for 2Ny, 2Nx <= 256 (the larger register
-// DFTs of longer lines do not fit the caps).
+// latency-bound at 14-16 resident warps: complex64 at 64 registers (4 blocks of 256 threads), FP64 at 128
+// (4 blocks of 128 threads, so only for 8 lines per CTA).  Measured per apply at 128x128x32: complex64 passes
+// 88 -> 77 us, FP64 139 -> 128 us; tighter caps spill and lose (FP64 at 96 registers, 5 blocks: k_fx spilled
+// 36 bytes and the whole FP64 apply took 0.320 against 0.312 ms).  Used for 2Ny, 2Nx <= 256 (the larger
+// register DFTs of longer lines do not fit the caps).
 template <typename R, int CAP> struct PassLB { static constexpr int T = kThreads, B = 1; };
 template <> struct PassLB<float, 1> { static constexpr int T = 256, B = 4; };
-template <> struct PassLB<double, 1> { static constexpr int T = 128, B = 5; };
+template <> struct PassLB<double, 1> { static constexpr int T = 128, B = 4; };
 
 // The vectors of one apply: nv = 1, or nv = 2 right-hand sides of the same operator that share every
 // tensor read.  Line zc of a pass runs over [0, nv*3Nz): vector zc / 3Nz, row zc % 3Nz.
