@@ -402,14 +402,15 @@ def run_b200(args, rank, world, local_rank):
         dt = torch.complex128 if prec == 0 else torch.complex64
         x = torch.randn(n, dtype=dt, device=dev)
         y = torch.empty_like(x)
-        for _ in range(3):
-            op.apply_device(x.data_ptr(), y.data_ptr(), prec)
         torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(reps):
-            op.apply_device(x.data_ptr(), y.data_ptr(), prec)
-        a1.record(stream)
+        with torch.cuda.stream(stream):  # back-to-back applies, no wait on another stream between them
+            for _ in range(3):
+                op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(reps):
+                op.apply_device(x.data_ptr(), y.data_ptr(), prec)
+            a1.record(stream)
         torch.cuda.synchronize()
         return a0.elapsed_time(a1) / reps
 
@@ -420,14 +421,15 @@ def run_b200(args, rank, world, local_rank):
         xs = [torch.randn(n, dtype=torch.complex64, device=dev) for _ in range(2)]
         ys = [torch.empty_like(x) for x in xs]
         pi, po = [x.data_ptr() for x in xs], [y.data_ptr() for y in ys]
-        for _ in range(3):
-            g2.apply_device_batch(op, pi, po, 1)
         torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(reps):
-            g2.apply_device_batch(op, pi, po, 1)
-        a1.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                g2.apply_device_batch(op, pi, po, 1)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(reps):
+                g2.apply_device_batch(op, pi, po, 1)
+            a1.record(stream)
         torch.cuda.synchronize()
         return a0.elapsed_time(a1) / reps
 
@@ -631,14 +633,15 @@ def run_apply_only(args):
         else:
             op.apply_device(x.data_ptr(), y.data_ptr(), args.prec)
 
-    for _ in range(args.warmup):
-        one()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.reps):
-        one()
-    e1.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            one()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.reps):
+            one()
+        e1.record(stream)
     torch.cuda.synchronize()
     op.check_device_error()
     form = 2 if args.nv == 2 else args.prec

@@ -16,6 +16,8 @@ from __future__ import annotations
 
 import ctypes
 import os
+import sys
+from contextlib import contextmanager
 from dataclasses import dataclass
 
 import numpy as np
@@ -205,6 +207,31 @@ def _c128(a):
     return np.ascontiguousarray(a, dtype=np.complex128)
 
 
+@contextmanager
+def _torch_ordered(stream_ptr):
+    """Order a device-pointer call on a library stream against torch's current stream.
+
+    The library's streams are non-blocking: they do not wait for torch's work, so a call whose inputs
+    were just written by torch (a dtype conversion, a copy, randn) could read them half-written, and
+    torch could read the call's outputs before they are complete.  On entry the library stream waits for
+    torch's current stream; on exit torch's current stream waits for the library stream.  Both are
+    device-side waits (events), the host does not block.  Without torch, before torch has set up CUDA,
+    or when torch's current stream is the library stream itself, nothing is done here (the C ABI's
+    contract: the caller orders its own work)."""
+    torch = sys.modules.get("torch")
+    pair = None
+    if torch is not None and torch.cuda.is_initialized():
+        cur = torch.cuda.current_stream()
+        if cur.cuda_stream != stream_ptr:
+            pair = (cur, torch.cuda.ExternalStream(stream_ptr))
+            pair[1].wait_stream(pair[0])
+    try:
+        yield
+    finally:
+        if pair is not None:
+            pair[0].wait_stream(pair[1])
+
+
 @dataclass
 class SolveInfo:
     iterations: int
@@ -306,7 +333,8 @@ class IEOperator:
         return vo
 
     def apply_device(self, d_in: int, d_out: int, precision: int = 0):
-        _check(lib().giem2g_apply_ie_operator_device(self.handle, d_in, d_out, precision), "apply_device")
+        with _torch_ordered(self.stream):
+            _check(lib().giem2g_apply_ie_operator_device(self.handle, d_in, d_out, precision), "apply_device")
 
     def contract_variants(self, precision: int) -> int:
         return lib().giem2g_contract_variants(self.handle, precision)
@@ -329,7 +357,8 @@ class IEOperator:
 
     def apply_preconditioner(self, d_v: int, d_z: int):
         """giem2g_apply_preconditioner: d_z = the registered network's guess of A^-1 v (device pointers)."""
-        _check(lib().giem2g_apply_preconditioner(self.handle, d_v, d_z), "apply_preconditioner")
+        with _torch_ordered(self.stream):
+            _check(lib().giem2g_apply_preconditioner(self.handle, d_v, d_z), "apply_preconditioner")
 
     def preconditioner_calls(self) -> int:
         return int(lib().giem2g_preconditioner_calls(self.handle))
@@ -382,8 +411,10 @@ class IEOperator:
     def solve_device(self, d_ebkg: int, d_esol: int, d_e0=None, tol=1e-8, max_restart=100, outer_buf=30,
                      inner_buf=10, precision=0):
         r = ResultT()
-        rc = lib().giem2g_solve_device(self.handle, d_ebkg, d_esol, d_e0,
-                                       self._ctl(tol, max_restart, outer_buf, inner_buf, precision), ctypes.byref(r))
+        with _torch_ordered(self.stream):
+            rc = lib().giem2g_solve_device(self.handle, d_ebkg, d_esol, d_e0,
+                                           self._ctl(tol, max_restart, outer_buf, inner_buf, precision),
+                                           ctypes.byref(r))
         _check(rc, "giem2g_solve_device")
         return self._info(r)
 
@@ -503,7 +534,8 @@ class RCOperator:
         return Ea, Ha
 
     def recalculate_device(self, d_E: int, d_Ea: int, d_Ha: int):
-        _check(lib().giem2g_rc_recalculate_device(self.handle, d_E, d_Ea, d_Ha), "giem2g_rc_recalculate_device")
+        with _torch_ordered(self.stream):
+            _check(lib().giem2g_rc_recalculate_device(self.handle, d_E, d_Ea, d_Ha), "giem2g_rc_recalculate_device")
 
     @property
     def stream(self) -> int:
@@ -552,7 +584,8 @@ class Batch:
         """Device pointers (lists of ints); returns a list of SolveInfo."""
         res = (ResultT * self.n)()
         e0 = _ptrs(d_e0) if d_e0 is not None else None
-        rc = lib().giem2g_batch_solve_device(self.handle, _ptrs(d_ebkg), _ptrs(d_esol), e0, self._ctl(tol), res)
+        with _torch_ordered(self.ops[0].stream):  # the batch runs on its first operator's stream
+            rc = lib().giem2g_batch_solve_device(self.handle, _ptrs(d_ebkg), _ptrs(d_esol), e0, self._ctl(tol), res)
         _check(rc, "giem2g_batch_solve_device")
         return [self._info(i, res[i]) for i in range(self.n)]
 
@@ -594,8 +627,9 @@ class Batch:
 
 def apply_device_batch(op, d_in, d_out, precision=1):
     """giem2g_apply_ie_operator_device_batch over lists of device pointers."""
-    _check(lib().giem2g_apply_ie_operator_device_batch(op.handle, len(d_in), _ptrs(d_in), _ptrs(d_out), precision),
-           "apply_device_batch")
+    with _torch_ordered(op.stream):
+        _check(lib().giem2g_apply_ie_operator_device_batch(op.handle, len(d_in), _ptrs(d_in), _ptrs(d_out),
+                                                           precision), "apply_device_batch")
 
 
 def gemm_bf16_tn(A, B, C=None, accumulate=False, err=None, stream=None):

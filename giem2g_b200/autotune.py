@@ -18,16 +18,19 @@ import os
 def _time_rounds(run, stream, reps: int, rounds: int) -> float:
     """Fastest of `rounds` CUDA-event timings of `reps` calls of run() (ms per call), after 2 warm-up calls."""
     import torch
-    for _ in range(2):
-        run()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):  # the calls run back to back on the operator's stream
+        for _ in range(2):
+            run()
     best = None
     for _ in range(rounds):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(reps):
-            run()
-        e1.record(stream)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                run()
+            e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         best = ms if best is None else min(best, ms)

@@ -122,7 +122,11 @@ int giem2g_set_fft_lines_precision(void *ie, int precision, int lines);
  * its contraction launch; giem2g_last_contract_ms returns the last one (ms, -1 if none). */
 int giem2g_set_kernel_timing(void *ie, int on);
 double giem2g_last_contract_ms(void *ie);
-/* CUDA stream the operator's kernels run on (cudaStream_t). */
+/* CUDA stream the operator's kernels run on (cudaStream_t).  It is created non-blocking, so it does
+ * not wait for the legacy default stream: every call that takes device pointers is ordered after
+ * earlier work on this stream only.  A caller whose inputs come from another stream makes this stream
+ * wait for them (cudaStreamWaitEvent) before the call, and makes its consumers wait for this stream
+ * after it (the Python layer, giem2g_b200, does both against torch's current stream). */
 void *giem2g_get_stream(void *ie);
 /* Milliseconds of device time of the last device apply (CUDA events), and kernels it launched. */
 double giem2g_last_apply_ms(void *ie);

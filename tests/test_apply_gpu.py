@@ -82,6 +82,29 @@ def test_apply_complex64_device(g2lib, orc):
     op.delete()
 
 
+def test_device_apply_follows_torch_stream(g2lib, orc):
+    """A device-pointer apply waits for the torch work that wrote its input, and torch waits for its
+    output.  Torch's stream spins for about 20 ms before it converts the input to complex64; the apply,
+    issued at once on the operator's non-blocking stream, still reads the converted vector, and torch
+    reads the result with no synchronisation in between."""
+    import torch
+    m, sig = config_small_block()
+    symm, asym = orc.green_tensor(m)
+    op, csiga, csigb, sqsigb = _setup(g2lib, orc, m, symm, asym, sig)
+    sh_o, ah_o = orc.tensor_spectrum(m.Nx, m.Ny, m.Nz, symm, asym)
+    v = random_vec(m, 7)
+    out_o = orc.apply(m.Nx, m.Ny, m.Nz, sh_o, ah_o, csiga, csigb, sqsigb, m.dz, v)
+    dv64 = torch.from_numpy(v.ravel()).cuda()
+    torch.cuda.synchronize()
+    torch.cuda._sleep(40_000_000)  # a bounded spin of 4e7 clock cycles on torch's current stream
+    dv = dv64.to(torch.complex64)
+    do = torch.empty_like(dv)
+    op.apply_device(dv.data_ptr(), do.data_ptr(), precision=1)
+    got = do.cpu().numpy()
+    assert rel(got.reshape(v.shape), out_o) < TOL32
+    op.delete()
+
+
 @pytest.mark.parametrize("shape", [(4, 4, 8), (8, 4, 16), (4, 4, 32), (2, 4, 48)])
 def test_complex64_specialised_and_generic_contraction(g2lib, orc, shape, monkeypatch):
     """complex64 path for the specialised Nz kernels and the generic kernel give the oracle's result."""
